@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark: 30-qubit complex128 random U3 + CNOT brickwork (20 layers) on one B200.
+
+One step = one full execution of the circuit from |0...0> through the engine's
+Circuit::execute path (lq_apply_circuit, fused passes).  The metric is the
+gate-layer bandwidth: the algorithmic bytes of every gate (U3 reads and writes
+the state, 2S; CNOT reads and writes the half it permutes, S; S = 16 * 2^n)
+divided by the step time.  The dominant kernel (the fused block pass) is
+reported against the measured HBM peak with its own algorithmic bytes (one
+read and one write of the state per launch).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the dense single-state simulation does not shard in this build;
+`--gpus N` (under torchrun) runs N independent replicas, one per GPU, and
+reports the whole-job aggregate (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0  # GB/s, earlier measurement on this pool
+
+
+def hbm_peak():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm = float(parts[1])
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            sms.append(sm)
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (restated reference loops) on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample_gates(n: int):
+    """A bounded sample of layer 0 of the brickwork with the layer's 2:1 mix of
+    U3 to CNOT: U3 on qubits 0..7 then CNOT(0,1), (2,3), (4,5), (6,7)."""
+    from logosq_b200 import workloads
+    g = workloads.brickwork_u3(n, 1, seed=2)
+    u3 = g[:8]
+    cx = g[n:n + 4]
+    return np.concatenate([u3, cx])
+
+
+def run_cpu_baseline(n: int, threads: int, repeats: int = 1):
+    import oracle
+    from logosq_b200 import abi
+    oracle.set_threads(threads)
+    g = cpu_sample_gates(n)
+    S = 16 << n
+    nbytes = sum(2 * S if r["kind"] == abi.U3 else S for r in g)
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    psi[0] = 1.0
+    # touch pages before timing
+    psi[::4096] = psi[::4096]
+    best = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        oracle.apply_circuit(psi, g)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    oracle.set_threads(1)
+    return nbytes / best / 1e9, best, len(g)
+
+
+# ---------------------------------------------------------------------------
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--per-gate-steps", type=int, default=1)
+    args = ap.parse_args()
+    n, layers = args.qubits, args.layers
+    ws, rank, local = dist_info()
+    metric = f"{n}q gate-layer GB/s"
+    config = {"workload": f"random U3+CNOT brickwork, {n} qubits complex128, {layers} layers, "
+                          f"seed 2, from |0...0>",
+              "qubits": n, "layers": layers, "state_bytes": 16 << n,
+              "l2_policy": "inputs larger than L2 (state 16 GiB >> 126 MB L2)" if n >= 24 else
+              "state fits L2",
+              "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        gbs, secs, ng = run_cpu_baseline(n, threads)
+        line = {"impl": "reference", "metric": metric, "value": gbs, "unit": "GB/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "dtype": "f64 (complex128)", "data": "synthetic",
+                "config": config, "vs_baseline": None,
+                "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+                                 "sample": f"{ng} gates of layer 0 ({ng * 2 // 3} U3 + "
+                                           f"{ng // 3} CNOT) at {n} qubits, {secs:.1f} s"},
+                "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    from logosq_b200 import State, abi, workloads
+    from logosq_b200._lib import call, lib
+
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    call("lq_set_device", local)
+
+    gates = workloads.brickwork_u3(n, layers, seed=2)
+    algo_bytes = workloads.brickwork_bytes(n, layers)
+    S = 16 << n
+    st = State.zero_state(n)
+    sp = C.c_void_p()
+    call("lq_state_stream", st.handle, C.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value)
+
+    def step():
+        call("lq_state_set_basis", st.handle, C.c_uint64(0))
+        call("lq_apply_circuit", st.handle, n, abi.gate_ptr(gates), len(gates), None, 0,
+             abi.EXEC_FUSED)
+
+    for _ in range(args.warmup):
+        step()
+    st.synchronize()
+    launches, passes = C.c_int(), C.c_int()
+    call("lq_last_circuit_stats", st.handle, C.byref(launches), C.byref(passes))
+
+    # ---- timed region (device time, CUDA events on the engine's stream) ----
+    call("lq_profile_enable", 1)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[local])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
+                           else local)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms_total = ev0.elapsed_time(ev1)
+    fused_ms, fused_n = C.c_double(), C.c_longlong()
+    call("lq_profile_read", 0, C.byref(fused_ms), C.byref(fused_n))
+    call("lq_profile_enable", 0)
+    if ws > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = ws * algo_bytes / (ms_step / 1e3) / 1e9
+
+    peak, peak_kind = hbm_peak()
+    fused_launch_ms = fused_ms.value / max(fused_n.value, 1)
+    achieved = 2 * S / (fused_launch_ms / 1e3) / 1e9 if fused_n.value else None
+    roofline = {"kernel": "k_fused_pass (TMA-staged 2^12-amplitude tiles)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": 2 * S, "avg_launch_ms": fused_launch_ms,
+                "launches_per_step": passes.value,
+                "traffic": None, "traffic_note": "see profiles/ (ncu dram bytes per launch)"}
+
+    # ---- per-gate (unfused) path: one sweep per gate, as Gate::apply --------
+    per_gate = None
+    if args.per_gate_steps > 0:
+        call("lq_profile_enable", 1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.per_gate_steps):
+            call("lq_state_set_basis", st.handle, C.c_uint64(0))
+            call("lq_apply_circuit", st.handle, n, abi.gate_ptr(gates), len(gates), None, 0,
+                 abi.EXEC_PER_GATE)
+        e1.record(stream)
+        e1.synchronize()
+        g_ms, g_n = C.c_double(), C.c_longlong()
+        call("lq_profile_read", 1, C.byref(g_ms), C.byref(g_n))
+        call("lq_profile_enable", 0)
+        pg_ms = e0.elapsed_time(e1) / args.per_gate_steps
+        per_gate = {"value": algo_bytes / (pg_ms / 1e3) / 1e9, "unit": "GB/s",
+                    "ms_per_step": pg_ms, "frac_of_hbm_peak": algo_bytes / (pg_ms / 1e3) / 1e9 / peak,
+                    "launches_per_step": int(g_n.value // max(args.per_gate_steps, 1))}
+
+    # ---- end to end through the public API, host buffers ----------------------
+    e2e = None
+    if not args.no_e2e:
+        host_gates = np.empty_like(gates)
+        pinned = torch.empty(2 << n, dtype=torch.float64, pin_memory=True)
+        pinned_ptr = C.cast(pinned.data_ptr(), C.POINTER(C.c_double))
+        torch.cuda.synchronize()
+        e2e_steps = max(1, min(args.steps, 3))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            host_gates[:] = gates  # the step's input lives in host memory
+            call("lq_state_set_basis", st.handle, C.c_uint64(0))
+            call("lq_apply_circuit", st.handle, n, abi.gate_ptr(host_gates), len(host_gates),
+                 None, 0, abi.EXEC_FUSED)
+            call("lq_state_download", st.handle, pinned_ptr, C.c_size_t(1 << n))
+        dt = (time.perf_counter() - t0) / e2e_steps
+        if ws > 1:
+            t = torch.tensor([dt], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": ws * algo_bytes / dt / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": int(gates.nbytes), "d2h_bytes_per_step": int(S),
+               "s_per_step": dt, "result": "final state vector downloaded to pinned host memory"}
+        del pinned
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        gbs, secs, ng = run_cpu_baseline(n, threads)
+        cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"{ng} gates of layer 0 ({ng * 2 // 3} U3 + {ng // 3} CNOT) at {n} "
+                         f"qubits, threaded restatement of the reference loops, {secs:.1f} s"}
+
+    gpu_launches = args.steps * (launches.value + 1)
+    line = {"metric": metric, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)",
+            "data": "synthetic (seeded)", "config": config,
+            "frac_of_hbm_peak_effective": value / peak,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "per_gate_path": per_gate,
+            "gpu_launches": gpu_launches, "clocks": clocks,
+            "fused_passes_per_step": passes.value}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    st.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

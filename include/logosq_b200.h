@@ -1,0 +1,326 @@
+/*
+ * logosq_b200.h -- C ABI of the B200 dense state-vector engine for LogosQ.
+ *
+ * The engine replaces the CPU dense path of LogosQ (`State` + `Gate::apply` +
+ * `Circuit::execute`, plus `Observable::expectation` and
+ * `GradientMethod::compute_gradient`) with hand-written sm_100a kernels.  Every
+ * entry point is `extern "C"`, takes plain pointers and sizes, returns an `int`
+ * status (LQ_OK on success) and never throws or aborts.  The text of the last
+ * failure on the calling thread is returned by lq_last_error().
+ *
+ * Conventions shared with the reference:
+ *   - Qubit q of an n-qubit state is bit (n-1-q) of the basis index (qubit 0 is
+ *     the most significant bit), as in src/gates/utils.rs:4-7.
+ *   - Amplitudes are complex numbers stored as interleaved (re, im) pairs,
+ *     like ndarray::Array1<Complex64> (src/states/mod.rs:38-41).
+ *   - Host buffers are owned by the caller; transfers are synchronous.
+ *
+ * Threading: a state handle is used by one host thread at a time (each handle
+ * owns one CUDA stream); distinct handles may be used concurrently.
+ */
+#ifndef LOGOSQ_B200_H
+#define LOGOSQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Status codes.  The first six mirror LogosQError (src/error.rs:9-61).
+ * ------------------------------------------------------------------------- */
+enum {
+    LQ_OK = 0,
+    LQ_ERR_QUBIT_INDEX = 1,        /* InvalidQubitIndex        src/error.rs:11-13 */
+    LQ_ERR_STATE_DIMENSION = 2,    /* InvalidStateDimension    src/error.rs:15-17 */
+    LQ_ERR_DIMENSION_MISMATCH = 3, /* DimensionMismatch        src/error.rs:19-21 */
+    LQ_ERR_GATE_MATRIX = 4,        /* InvalidGateMatrix        src/error.rs:23-28 */
+    LQ_ERR_PARAM_COUNT = 5,        /* ParameterCountMismatch   src/error.rs:30-32 */
+    LQ_ERR_QUBIT_MISMATCH = 6,     /* CircuitQubitMismatch     src/error.rs:34-40 */
+    LQ_ERR_INVALID_ARG = 7,        /* null pointer, bad enum, bad size          */
+    LQ_ERR_OOM = 8,                /* device allocation refused                 */
+    LQ_ERR_CUDA = 9,               /* CUDA runtime or driver error              */
+    LQ_ERR_TIMEOUT = 10,           /* a bounded device wait ran out             */
+    LQ_ERR_UNSUPPORTED = 11        /* dtype / size not supported by this call   */
+};
+
+/* Amplitude storage type of a state. */
+enum {
+    LQ_C128 = 0, /* complex128 (2 x f64), the drop-in type (Complex64 in Rust) */
+    LQ_C64 = 1   /* complex64 (2 x f32), the tensor-core precision form        */
+};
+
+/* ---------------------------------------------------------------------------
+ * Gate descriptors.  One descriptor per reference gate struct / builder.
+ * ------------------------------------------------------------------------- */
+enum {
+    LQ_GATE_H = 0,        /* HGate            src/gates/single_qubit.rs:90-113          */
+    LQ_GATE_X = 1,        /* XGate            src/gates/single_qubit.rs:14-31           */
+    LQ_GATE_Y = 2,        /* YGate            src/gates/single_qubit.rs:39-58 (applies -Y,
+                             as the reference struct does)                               */
+    LQ_GATE_Z = 3,        /* ZGate            src/gates/single_qubit.rs:67-82           */
+    LQ_GATE_S = 4,        /* SGate            src/gates/single_qubit.rs:121-137         */
+    LQ_GATE_T = 5,        /* TGate            src/gates/single_qubit.rs:145-161         */
+    LQ_GATE_RX = 6,       /* RXGate           src/gates/parameterized.rs:48-80          */
+    LQ_GATE_RY = 7,       /* RYGate           src/gates/parameterized.rs:101-133        */
+    LQ_GATE_RZ = 8,       /* RZGate           src/gates/parameterized.rs:154-178        */
+    LQ_GATE_PHASE = 9,    /* PhaseGate        src/gates/parameterized.rs:199-218        */
+    LQ_GATE_U3 = 10,      /* U3Gate           src/gates/parameterized.rs:249-282        */
+    LQ_GATE_CNOT = 11,    /* CNOTGate         src/gates/two_qubit.rs:12-31              */
+    LQ_GATE_SWAP = 12,    /* SWAPGate         src/gates/two_qubit.rs:40-62              */
+    LQ_GATE_CZ = 13,      /* CZGate           src/gates/two_qubit.rs:71-92              */
+    LQ_GATE_CPHASE = 14,  /* CPhaseGate       src/gates/two_qubit.rs:100-134            */
+    LQ_GATE_TOFFOLI = 15, /* ToffoliGate      src/gates/three_qubit.rs:13-35            */
+    LQ_GATE_CRX = 16,     /* CRXGate          src/gates/parameterized.rs:311-343        */
+    LQ_GATE_CRY = 17,     /* CRYGate          src/gates/parameterized.rs:368-399        */
+    LQ_GATE_CRZ = 18,     /* CRZGate          src/gates/parameterized.rs:424-451        */
+    LQ_GATE_CPHASE_PARAM = 19, /* CPhaseParamGate src/gates/parameterized.rs:476-499   */
+    LQ_GATE_RXX = 20,     /* RXXGate          src/gates/parameterized.rs:528-580 (keeps the
+                             reference's |01>/|10> block rule, see LQ_FLAG_TEXTBOOK)     */
+    LQ_GATE_RYY = 21,     /* RYYGate          src/gates/parameterized.rs:604-655        */
+    LQ_GATE_RZZ = 22,     /* RZZGate          src/gates/parameterized.rs:679-709        */
+    LQ_GATE_MATRIX1 = 23, /* 2x2 matrix on q[0]: Circuit::h/x/y/z/s/t/r*_matrix
+                             (src/circuits/single_qubit.rs:12-126), lowered from the
+                             dense 2^n x 2^n MatrixGate to a single-qubit sweep          */
+    LQ_GATE_MATRIX2 = 24, /* 4x4 matrix on (q[0], q[1]) with q[0] the high bit of the
+                             4x4 index: Circuit::add_two_qubit_gate
+                             (src/circuits/two_qubits.rs:11-82)                          */
+    LQ_GATE__COUNT = 25
+};
+
+/* Descriptor flags. */
+enum {
+    LQ_FLAG_RENORM = 1,  /* normalize the state after this gate, as MatrixGate::apply
+                            does (src/gates/mod.rs:76-93)                                */
+    LQ_FLAG_TEXTBOOK = 2 /* RXX/RYY: apply the full 4x4 rotation instead of the
+                            reference's loop (which skips the |01>,|10> block when
+                            qubit1 < qubit2, src/gates/parameterized.rs:563-577)         */
+};
+
+/*
+ * One gate.  q[] holds LogosQ qubit indices (unused entries -1): the qubit for
+ * one-qubit gates, (control, target) or (qubit1, qubit2) for two-qubit gates,
+ * (control1, control2, target) for Toffoli.  angle[] is (theta, phi, lambda)
+ * for U3, (theta) for rotations and (angle) for CPhase.  If param[k] >= 0 the
+ * angle k is taken from the caller's parameter vector instead:
+ *     angle_k = theta[param[k]] * scale[k] + angle[k]
+ * which is how an Ansatz (src/optimization/ansatz.rs:10-43) is described once
+ * and re-bound to new parameter vectors.  m[] holds the matrix of MATRIX1
+ * (2x2) and MATRIX2 (4x4) gates, row-major, interleaved (re, im).
+ */
+typedef struct lq_gate {
+    int32_t kind;
+    int32_t flags;
+    int32_t q[3];
+    int32_t param[3];
+    double angle[3];
+    double scale[3];
+    double m[32];
+} lq_gate;
+
+/*
+ * One Pauli string P = X^x Z^z (up to phase) with a real coefficient, the
+ * packed form of PauliTerm (src/optimization/observable.rs:79-83).  xmask has
+ * bit (n-1-q) set when qubit q carries X or Y; zmask when it carries Z or Y;
+ * ny counts the Y factors.  Its expectation is
+ *     coefficient * Re sum_i conj(psi_i) * phase(i) * psi_{i ^ xmask},
+ *     phase(i) = (+-i)^ny * (-1)^popcount(i & zmask)
+ * with +i under LQ_Y_REFERENCE (the convention of PauliTerm::expectation,
+ * src/optimization/observable.rs:125-132) and -i under LQ_Y_TEXTBOOK.
+ */
+typedef struct lq_pauli_term {
+    double coefficient;
+    uint64_t xmask;
+    uint64_t zmask;
+    int32_t ny;
+    int32_t reserved;
+} lq_pauli_term;
+
+enum { LQ_Y_REFERENCE = 0, LQ_Y_TEXTBOOK = 1 };
+
+/* Execution modes of lq_apply_circuit. */
+enum {
+    LQ_EXEC_FUSED = 0,   /* plan the gate list into fused shared-memory block passes */
+    LQ_EXEC_PER_GATE = 1 /* one sweep per gate, in order (the Gate::apply path)      */
+};
+
+typedef struct lq_state lq_state;
+
+/* ---------------------------------------------------------------------------
+ * Library / device
+ * ------------------------------------------------------------------------- */
+/* Text of the last error raised on this host thread ("" if none). */
+const char *lq_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int lq_version(void);
+/* Number of visible CUDA devices. */
+int lq_device_count(int *count);
+/* Select the device that later lq_state_create calls on this thread use. */
+int lq_set_device(int device);
+/* Host-side cap on bytes that lq_state_create may allocate (0 = no cap).
+ * Lets tests exercise LQ_ERR_OOM without exhausting a shared GPU. */
+int lq_set_alloc_limit(uint64_t bytes);
+
+/* Launch timing (no reference counterpart; used by the benchmark): when
+ * enabled, CUDA events bracket every launch and lq_profile_read returns the
+ * summed device time and launch count of one kernel class:
+ * 0 fused block passes, 1 per-gate sweeps, 2 reductions, 3 batched engine,
+ * 4 tensor-core blocks.  Enabling (or disabling) resets the counters. */
+int lq_profile_enable(int on);
+int lq_profile_read(int kernel_class, double *total_ms, long long *launches);
+
+/* ---------------------------------------------------------------------------
+ * State (src/states/mod.rs:38-141)
+ * ------------------------------------------------------------------------- */
+/* Allocate an n-qubit state of the given dtype, initialised to |0...0>
+ * (State::zero_state, src/states/mod.rs:136-141). */
+int lq_state_create(int num_qubits, int dtype, lq_state **out);
+int lq_state_destroy(lq_state *s);
+int lq_state_num_qubits(const lq_state *s, int *out);
+int lq_state_dtype(const lq_state *s, int *out);
+/* |basis> : zero_state (index 0) and one_state (index 2^n-1), src/states/mod.rs:136-150 */
+int lq_state_set_basis(lq_state *s, uint64_t index);
+/* plus_state, src/states/mod.rs:153-158 */
+int lq_state_set_plus(lq_state *s);
+/* Copy num_amplitudes (must equal 2^n) interleaved complex128 values from the
+ * host (State::new without normalisation / vector_mut, src/states/mod.rs:55-133).
+ * For a C64 state the values are rounded to complex64 on the device. */
+int lq_state_upload(lq_state *s, const double *host, size_t num_amplitudes);
+int lq_state_download(const lq_state *s, double *host, size_t num_amplitudes);
+/* Same for complex64 host data (C64 states only). */
+int lq_state_upload_c64(lq_state *s, const float *host, size_t num_amplitudes);
+int lq_state_download_c64(const lq_state *s, float *host, size_t num_amplitudes);
+/* dst <- src (same n and dtype), like State::clone. */
+int lq_state_copy(lq_state *dst, const lq_state *src);
+/* out <- |a> (x) |b> (State::tensor_product, src/states/mod.rs:298-314);
+ * out must have n_a + n_b qubits. */
+int lq_state_tensor_product(lq_state *out, const lq_state *a, const lq_state *b);
+/* Wait for all work queued on the state's stream. */
+int lq_state_synchronize(lq_state *s);
+/* Device pointer and CUDA stream (cudaStream_t) of the state, for callers that
+ * interoperate with other CUDA code.  The pointer stays owned by the handle. */
+int lq_state_device_ptr(lq_state *s, void **dptr);
+int lq_state_stream(lq_state *s, void **stream);
+
+/* ---------------------------------------------------------------------------
+ * Reductions (FP64 accumulation for both dtypes)
+ * ------------------------------------------------------------------------- */
+/* sum |a_i|^2 */
+int lq_norm_sqr(const lq_state *s, double *out);
+/* State::normalize (src/states/mod.rs:91-114): divide by the norm if > 1e-10. */
+int lq_normalize(lq_state *s);
+/* State::probabilities (src/states/mod.rs:277-279): |a_i|^2 into host[2^n]. */
+int lq_probabilities(const lq_state *s, double *host, size_t len);
+/* State::probability (src/states/mod.rs:288-293): 0.0 when out of range. */
+int lq_probability(const lq_state *s, uint64_t basis, double *out);
+/* <a|b> = sum conj(a_i) b_i (inner_product_parallel, src/states/mod.rs:350-365);
+ * out[0] = re, out[1] = im. */
+int lq_inner_product(const lq_state *a, const lq_state *b, double out[2]);
+/* n_shots basis indices drawn from |a_i|^2 (measure / measure_shots_parallel,
+ * src/states/mod.rs:180-258) with a seeded counter-based generator. */
+int lq_measure_shots(const lq_state *s, uint64_t n_shots, uint64_t seed, uint64_t *host_out);
+/* sum_t coefficient_t * <P_t> (PauliObservable::expectation,
+ * src/optimization/observable.rs:228-232; PauliTerm::expectation :95-147).
+ * per_term (optional, may be NULL) receives each term's contribution. */
+int lq_expectation_pauli(const lq_state *s, const lq_pauli_term *terms, int nterms,
+                         int y_convention, double *out, double *per_term);
+
+/* ---------------------------------------------------------------------------
+ * Gates (src/gates/*.rs) -- each call is one in-place sweep on the state's
+ * stream, the drop-in for Gate::apply (src/gates/mod.rs:26-35).
+ * ------------------------------------------------------------------------- */
+/* One descriptor; theta may be NULL when no param[] index is used. */
+int lq_apply_gate(lq_state *s, const lq_gate *g, const double *theta, int ntheta);
+/* 2x2 matrix m (row-major, interleaved re/im) on one qubit. */
+int lq_apply_matrix1(lq_state *s, int qubit, const double m[8]);
+/* 2x2 matrix on target when control is |1> (CRX/CRY/CNOT family). */
+int lq_apply_controlled1(lq_state *s, int control, int target, const double m[8]);
+/* Diagonal gate on k <= 3 qubits: amplitude *= phases[pattern], pattern = the
+ * bits of the k qubits, qubits[0] most significant; phases has 2^k complex. */
+int lq_apply_diagonal(lq_state *s, int k, const int *qubits, const double *phases);
+/* SWAPGate (src/gates/two_qubit.rs:40-62). */
+int lq_apply_swap(lq_state *s, int qubit1, int qubit2);
+/* 4x4 matrix on (qubit1, qubit2), qubit1 the high bit of the 4x4 index. */
+int lq_apply_matrix2(lq_state *s, int qubit1, int qubit2, const double m[32]);
+/* MatrixGate::apply (src/gates/mod.rs:76-93): a full 2^n x 2^n matrix m
+ * (row-major, interleaved re/im, dim = 2^n, n <= 13) times the state, then
+ * State::normalize, exactly as the reference's dense gate does. */
+int lq_apply_dense(lq_state *s, const double *m, uint64_t dim);
+/* Dense 2^k x 2^k matrix (k <= 4) on the listed qubits (qubits[0] the high bit
+ * of the matrix index), applied by the fused shared-memory block kernel. */
+int lq_apply_block(lq_state *s, int k, const int *qubits, const double *m);
+
+/* ---------------------------------------------------------------------------
+ * Circuit::execute (src/circuits/mod.rs:352-375)
+ * ------------------------------------------------------------------------- */
+/* Apply ops[0..nops) in order.  LQ_EXEC_FUSED groups them into fused passes
+ * (each a TMA-staged shared-memory tile kernel); LQ_EXEC_PER_GATE runs one sweep
+ * per gate.  circuit_qubits must equal the state's qubit count
+ * (CircuitQubitMismatch, src/circuits/mod.rs:353-358). */
+int lq_apply_circuit(lq_state *s, int circuit_qubits, const lq_gate *ops, int nops,
+                     const double *theta, int ntheta, int mode);
+/* Host-only planning query (no device work): how lq_apply_circuit in fused
+ * mode would split the gate list on an n-qubit state -- number of fused passes
+ * (full-state HBM sweeps), register rounds inside them, and gates that run as
+ * standalone per-gate sweeps. */
+int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, int *rounds,
+                    int *standalone);
+/* Statistics of the last lq_apply_circuit on this handle: number of kernel
+ * launches and number of fused passes (0 in per-gate mode). */
+int lq_last_circuit_stats(const lq_state *s, int *launches, int *passes);
+
+/* ---------------------------------------------------------------------------
+ * Variational calls (src/optimization/)
+ * ------------------------------------------------------------------------- */
+/* Energy of |0> evolved by the parameterised gate list: the objective closure
+ * of VQE::run (src/optimization/vqe.rs:63-67).  work is any state handle with
+ * the right qubit count; it is overwritten. */
+int lq_ansatz_energy(lq_state *work, const lq_gate *ops, int nops, const double *theta,
+                     int nparams, const lq_pauli_term *terms, int nterms, int y_convention,
+                     double *energy);
+/* ParameterShift::compute_gradient (src/optimization/gradient.rs:44-78):
+ * grad_i = (E(theta + shift e_i) - E(theta - shift e_i)) / 2. */
+int lq_parameter_shift(lq_state *work, const lq_gate *ops, int nops, const double *theta,
+                       int nparams, const lq_pauli_term *terms, int nterms, int y_convention,
+                       double shift, double *grad);
+/* FiniteDifference::compute_gradient (src/optimization/gradient.rs:96-125). */
+int lq_finite_difference(lq_state *work, const lq_gate *ops, int nops, const double *theta,
+                         int nparams, const lq_pauli_term *terms, int nterms, int y_convention,
+                         double epsilon, double *grad);
+
+/* ---------------------------------------------------------------------------
+ * Batched parameter-shift engine: all 2P+1 circuits of many VQE instances of
+ * uneven qubit counts in one persistent, CUDA-graph-captured launch.
+ * ------------------------------------------------------------------------- */
+typedef struct lq_vqe_instance {
+    int32_t num_qubits;        /* 1..20 */
+    int32_t nops;
+    const lq_gate *ops;        /* parameterised ansatz (param[] indices into theta) */
+    int32_t nparams;
+    int32_t nterms;
+    const lq_pauli_term *terms;
+} lq_vqe_instance;
+
+typedef struct lq_batch lq_batch;
+
+/* Build the batch (copies every descriptor to the device, plans the work list
+ * and captures the launch in a CUDA graph on first use). */
+int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch **out);
+int lq_batch_destroy(lq_batch *b);
+/* Total parameter count over all instances. */
+int lq_batch_num_params(const lq_batch *b, int *out);
+/* theta: concatenated parameter vectors (instance order).  energy[ninstances]
+ * gets E(theta), grad[total params] the parameter-shift gradient. */
+int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *energy,
+                       double *grad);
+/* Tuning chosen by the batch autotuner: states per CTA tile limit and the
+ * fused-gate width used for shared-memory resident instances. */
+int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *threads_per_cta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOGOSQ_B200_H */

@@ -1,0 +1,177 @@
+"""CPU parity oracle for the LogosQ dense path -- TEST INFRASTRUCTURE ONLY.
+
+A C++ restatement of the reference's CPU loops (oracle/logosq_oracle.cpp),
+compiled with gcc into oracle/_build/liblogosq_oracle.so and called through
+ctypes.  Only the test suite, the smoke check and the CPU-baseline leg of the
+benchmark import this package; the product library never links or calls it.
+
+Parity pins: tests/test_oracle_golden.py checks this oracle against the
+known-answer assertions of the reference's own tests (read as text from the
+reference's tests/*.rs) and against numpy; see logosq_oracle.cpp's header.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from logosq_b200 import abi
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "logosq_oracle.cpp"
+BUILD = HERE / "_build"
+LIB = BUILD / "liblogosq_oracle.so"
+
+CXXFLAGS = ["-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared"]
+
+
+def build(force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    hdr = HERE.parent / "include" / "logosq_b200.h"
+    if force or not LIB.exists() or LIB.stat().st_mtime < max(SRC.stat().st_mtime,
+                                                                hdr.stat().st_mtime):
+        subprocess.run(["g++", *CXXFLAGS, str(SRC), "-o", str(LIB)], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        lb = C.CDLL(str(LIB))
+        PD, PG, PT = C.POINTER(C.c_double), C.POINTER(abi.LqGate), C.POINTER(abi.LqPauliTerm)
+        sig = {
+            "or_set_threads": (None, [C.c_int]),
+            "or_get_threads": (C.c_int, []),
+            "or_max_threads": (C.c_int, []),
+            "or_apply_gate": (None, [PD, C.c_int, PG, PD]),
+            "or_apply_circuit": (None, [PD, C.c_int, PG, C.c_int, PD]),
+            "or_normalize": (None, [PD, C.c_int]),
+            "or_norm_sqr": (C.c_double, [PD, C.c_int]),
+            "or_probabilities": (None, [PD, C.c_int, PD]),
+            "or_inner_product": (None, [PD, PD, C.c_int, PD]),
+            "or_pauli_term": (C.c_double, [PD, C.c_int, PT, C.c_int]),
+            "or_expectation": (C.c_double, [PD, C.c_int, PT, C.c_int, C.c_int]),
+            "or_heisenberg_energy": (C.c_double, [PD, C.c_int, C.c_double, C.c_double,
+                                                  C.c_double, C.c_double]),
+            "or_ansatz_energy": (C.c_double, [C.c_int, PG, C.c_int, PD, PT, C.c_int, C.c_int]),
+            "or_parameter_shift": (None, [C.c_int, PG, C.c_int, PD, C.c_int, PT, C.c_int, C.c_int,
+                                          C.c_double, PD]),
+            "or_finite_difference": (None, [C.c_int, PG, C.c_int, PD, C.c_int, PT, C.c_int,
+                                            C.c_int, C.c_double, PD]),
+            "or_vqe_adam": (C.c_int, [C.c_int, PG, C.c_int, PD, C.c_int, PT, C.c_int, C.c_int,
+                                      C.c_double, C.c_int, C.c_double, PD, PD]),
+            "or_apply_dense": (None, [PD, C.c_int, PD]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lb, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lb
+    return _lib
+
+
+def _pd(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_threads(t: int) -> None:
+    """1 = faithful mode (serial where the reference is serial); >1 threaded."""
+    lib().or_set_threads(int(t))
+
+
+def max_threads() -> int:
+    return lib().or_max_threads()
+
+
+def zero_state(n: int) -> np.ndarray:
+    v = np.zeros(1 << n, dtype=np.complex128)
+    v[0] = 1.0
+    return v
+
+
+def apply_circuit(psi: np.ndarray, gates: np.ndarray, theta=None) -> np.ndarray:
+    """In place on psi (complex128, contiguous); returns psi."""
+    assert psi.dtype == np.complex128 and psi.flags["C_CONTIGUOUS"]
+    n = int(np.log2(len(psi)))
+    th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float64)
+    lib().or_apply_circuit(_pd(psi.view(np.float64)), n, abi.gate_ptr(gates), len(gates),
+                           None if th is None else _pd(th))
+    return psi
+
+
+def normalize(psi):
+    lib().or_normalize(_pd(psi.view(np.float64)), int(np.log2(len(psi))))
+    return psi
+
+
+def norm_sqr(psi) -> float:
+    return lib().or_norm_sqr(_pd(psi.view(np.float64)), int(np.log2(len(psi))))
+
+
+def probabilities(psi):
+    out = np.empty(len(psi), dtype=np.float64)
+    lib().or_probabilities(_pd(psi.view(np.float64)), int(np.log2(len(psi))), _pd(out))
+    return out
+
+
+def inner_product(a, b) -> complex:
+    out = np.zeros(2)
+    lib().or_inner_product(_pd(a.view(np.float64)), _pd(b.view(np.float64)),
+                           int(np.log2(len(a))), _pd(out))
+    return complex(out[0], out[1])
+
+
+def expectation(psi, terms: np.ndarray, y_convention: int = abi.Y_REFERENCE) -> float:
+    return lib().or_expectation(_pd(psi.view(np.float64)), int(np.log2(len(psi))),
+                                abi.term_ptr(terms), len(terms), y_convention)
+
+
+def heisenberg_energy(psi, jx, jy, jz, h) -> float:
+    return lib().or_heisenberg_energy(_pd(psi.view(np.float64)), int(np.log2(len(psi))),
+                                      jx, jy, jz, h)
+
+
+def ansatz_energy(n, gates, theta, terms, y_convention=abi.Y_REFERENCE) -> float:
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    return lib().or_ansatz_energy(n, abi.gate_ptr(gates), len(gates), _pd(th), abi.term_ptr(terms),
+                                  len(terms), y_convention)
+
+
+def parameter_shift(n, gates, theta, terms, shift=np.pi / 2, y_convention=abi.Y_REFERENCE):
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    g = np.zeros(len(th))
+    lib().or_parameter_shift(n, abi.gate_ptr(gates), len(gates), _pd(th), len(th),
+                             abi.term_ptr(terms), len(terms), y_convention, shift, _pd(g))
+    return g
+
+
+def finite_difference(n, gates, theta, terms, eps=1e-7, y_convention=abi.Y_REFERENCE):
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    g = np.zeros(len(th))
+    lib().or_finite_difference(n, abi.gate_ptr(gates), len(gates), _pd(th), len(th),
+                               abi.term_ptr(terms), len(terms), y_convention, eps, _pd(g))
+    return g
+
+
+def vqe_adam(n, gates, theta0, terms, lr=0.1, max_iter=100, tol=1e-6,
+             y_convention=abi.Y_REFERENCE):
+    th = np.array(theta0, dtype=np.float64)
+    hist = np.zeros(max_iter + 1)
+    fv = C.c_double()
+    k = lib().or_vqe_adam(n, abi.gate_ptr(gates), len(gates), _pd(th), len(th),
+                          abi.term_ptr(terms), len(terms), y_convention, lr, max_iter, tol,
+                          _pd(hist), C.byref(fv))
+    return th, fv.value, hist[:k]
+
+
+def apply_dense(psi, matrix):
+    m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128))
+    lib().or_apply_dense(_pd(psi.view(np.float64)), int(np.log2(len(psi))),
+                         _pd(m.view(np.float64)))
+    return psi
