@@ -151,6 +151,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--per-gate-steps", type=int, default=1)
+    ap.add_argument("--fusion-width", type=int, default=0,
+                    help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
     args = ap.parse_args()
     n, layers = args.qubits, args.layers
     ws, rank, local = dist_info()
@@ -202,6 +204,26 @@ def main():
         call("lq_apply_circuit", st.handle, n, abi.gate_ptr(gates), len(gates), None, 0,
              abi.EXEC_FUSED)
 
+    # Autotune the fusion width (tile bits) on this workload: one timed step per
+    # candidate after a first warm-up step, keep the fastest.
+    tune = {}
+    if args.fusion_width:
+        call("lq_set_fusion_width", args.fusion_width)
+    else:
+        step()
+        st.synchronize()
+        for T in (10, 11, 12):
+            call("lq_set_fusion_width", T)
+            t0 = time.perf_counter()
+            step()
+            st.synchronize()
+            tune[T] = time.perf_counter() - t0
+        call("lq_set_fusion_width", min(tune, key=tune.get))
+    fw = C.c_int()
+    call("lq_get_fusion_width", C.byref(fw))
+    config["fusion_width_tile_bits"] = fw.value
+    if tune:
+        config["autotune_s_per_step"] = {str(k): round(v, 4) for k, v in tune.items()}
     for _ in range(args.warmup):
         step()
     st.synchronize()

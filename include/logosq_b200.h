@@ -261,12 +261,23 @@ int lq_apply_block(lq_state *s, int k, const int *qubits, const double *m);
  * (CircuitQubitMismatch, src/circuits/mod.rs:353-358). */
 int lq_apply_circuit(lq_state *s, int circuit_qubits, const lq_gate *ops, int nops,
                      const double *theta, int ntheta, int mode);
+/* Fusion width of lq_apply_circuit: tile bits T (5..12) of a fused pass,
+ * i.e. 2^T amplitudes staged per CTA.  Chosen by the benchmark's autotuner;
+ * default 11. */
+int lq_set_fusion_width(int tile_bits);
+int lq_get_fusion_width(int *tile_bits);
 /* Host-only planning query (no device work): how lq_apply_circuit in fused
  * mode would split the gate list on an n-qubit state -- number of fused passes
  * (full-state HBM sweeps), register rounds inside them, and gates that run as
  * standalone per-gate sweeps. */
 int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, int *rounds,
                     int *standalone);
+/* Host-only dump of the fused program lq_apply_circuit would run (for tests and
+ * inspection): int32 counts {steps, rounds, ops, coefficients, T}, then per
+ * step int32 {fused, gate, h, round_begin, nrounds}, the round records, the op
+ * records and the FP64 coefficients.  *used receives the size needed. */
+int lq_plan_dump(int num_qubits, const lq_gate *ops, int nops, const double *theta, int ntheta,
+                 void *buf, size_t cap, size_t *used);
 /* Statistics of the last lq_apply_circuit on this handle: number of kernel
  * launches and number of fused passes (0 in per-gate mode). */
 int lq_last_circuit_stats(const lq_state *s, int *launches, int *passes);

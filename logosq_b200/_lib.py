@@ -74,6 +74,10 @@ _PROTOS = {
     "lq_apply_circuit": (C.c_int, [_P, C.c_int, _PG, C.c_int, _PD, C.c_int, C.c_int]),
     "lq_last_circuit_stats": (C.c_int, [_P, _PI, _PI]),
     "lq_plan_circuit": (C.c_int, [C.c_int, _PG, C.c_int, _PI, _PI, _PI]),
+    "lq_set_fusion_width": (C.c_int, [C.c_int]),
+    "lq_get_fusion_width": (C.c_int, [_PI]),
+    "lq_plan_dump": (C.c_int, [C.c_int, _PG, C.c_int, _PD, C.c_int, _P, C.c_size_t,
+                               C.POINTER(C.c_size_t)]),
     "lq_ansatz_energy": (C.c_int, [_P, _PG, C.c_int, _PD, C.c_int, _PT, C.c_int, C.c_int, _PD]),
     "lq_parameter_shift": (
         C.c_int, [_P, _PG, C.c_int, _PD, C.c_int, _PT, C.c_int, C.c_int, C.c_double, _PD]),

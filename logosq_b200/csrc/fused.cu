@@ -1,268 +1,57 @@
 // Fused k-qubit block passes: Circuit::execute (src/circuits/mod.rs:352-375)
 // without one full-state sweep per gate.
 //
-// A pass owns a set W of T <= 12 index bits: the four lowest bits (so every
+// A pass owns a window W of T <= 12 index bits: the four lowest bits (so every
 // global access is a 256-byte contiguous run) plus a contiguous range
-// [h, h+T-4).  Each CTA stages one 2^T-amplitude tile (64 KiB of complex128 at
-// T = 12) from HBM into shared memory with one TMA tensor copy (128-byte
-// swizzle), applies every gate of the pass that acts inside W, and writes the
-// tile back with one TMA store.  Inside the CTA the gates run in "rounds": a
-// round picks four tile bits R, each thread gathers the 16 amplitudes that
-// differ only in R into registers, applies all of the round's gates there, and
-// scatters them back.  HBM traffic per pass is one read and one write of the
-// state, however many gates the pass holds.
+// [h, h+T-4).  A persistent CTA walks the 2^(n-T) tiles of the state; each
+// tile (2^T amplitudes, 32 KiB of complex128 at T = 11) is staged from HBM
+// into shared memory by one TMA tensor copy (128-byte swizzle) while the CTA
+// computes on the previous tile (two buffers), every gate of the pass is
+// applied, and the tile goes back by an asynchronous TMA store.  HBM traffic
+// per pass is one read and one write of the state, however many gates the
+// pass holds.
+//
+// Inside the CTA the gates run in "rounds" (fused_core.cuh): a round picks four
+// tile bits R, each thread gathers the 16 amplitudes that differ only in R
+// into registers, applies the round's gates there, and scatters them back.
+// Only the bits a gate mixes or permutes (its target; both bits of a SWAP or
+// 4x4) must be in R.  Control bits and every bit of a diagonal gate may lie
+// anywhere -- in R, elsewhere in the tile (constant per thread during a round)
+// or outside the window (constant per tile during the pass): their values are
+// read from the thread's global basis index.  So CNOT controls, CPhase, CZ, RZ
+// and RZZ fuse into any pass that holds their target (diagonal gates need none).
 //
 // The planner (host) picks windows greedily: at each step it chooses the h
 // that lets the most not-yet-applied gates run (respecting gate order per
-// bit), then splits that pass into register rounds.  Gates that fit no window
-// (two-qubit gates whose bits are further apart than the window) and gates
+// bit), then splits that pass into register rounds.  Gates whose mixed bits fit
+// no window (a SWAP or 4x4 on bits further apart than the window) and gates
 // that renormalise run as standalone per-gate sweeps at their place in order.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
-#include "gate_ops.h"
+#include "fused_plan.h"
 
 namespace lq {
 
-// ---------------------------------------------------------------------------
-// Device program of a pass
-// ---------------------------------------------------------------------------
-enum FusedOpType {
-    F_M1 = 0,     // 2x2 on reg bit k0, controls: reg-bit mask cm (all set)
-    F_PERM1 = 1,  // X on reg bit k0, controls cm
-    F_DIAG = 2,   // phases on pattern reg bits (k0 lsb, k1), fix mask cm
-    F_SWAP = 3,   // swap reg bits k0, k1
-    F_M2 = 4,     // 4x4, index = bit(k0)<<1 | bit(k1)
-    F_BLOCK3 = 5, // 8x8 on reg bits 0..2 (matrix bit j <-> reg bit j)
-    F_BLOCK4 = 6  // 16x16 on reg bits 0..3
-};
-
-struct FusedOp {
-    int32_t type;
-    int32_t k0, k1, npat;
-    int32_t cm;       // control / fix mask over register bits
-    int32_t coef;     // offset of the coefficients in the coefficient array (doubles)
-};
-
-struct FusedRound {
-    int32_t rpos[4];   // tile-local bit positions of register bits 0..3
-    int32_t lane[12];  // tile-local positions of thread-index bits, in order
-    int32_t nlane;
-    int32_t op_begin, op_end;
-    int32_t pad;
-};
-
-constexpr int kMaxT = 12;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
-
-template <int K>
-__device__ __forceinline__ void reg_m1(double2 (&a)[16], int cm, const double *__restrict__ c) {
-    const double m00r = c[0], m00i = c[1], m01r = c[2], m01i = c[3];
-    const double m10r = c[4], m10i = c[5], m11r = c[6], m11i = c[7];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if (e & (1 << K)) continue;
-        if ((e & cm) != cm) continue;
-        const double2 a0 = a[e], a1 = a[e | (1 << K)];
-        double2 o0, o1;
-        o0.x = (m00r * a0.x - m00i * a0.y) + (m01r * a1.x - m01i * a1.y);
-        o0.y = (m00r * a0.y + m00i * a0.x) + (m01r * a1.y + m01i * a1.x);
-        o1.x = (m10r * a0.x - m10i * a0.y) + (m11r * a1.x - m11i * a1.y);
-        o1.y = (m10r * a0.y + m10i * a0.x) + (m11r * a1.y + m11i * a1.x);
-        a[e] = o0;
-        a[e | (1 << K)] = o1;
-    }
-}
-
-template <int K>
-__device__ __forceinline__ void reg_perm1(double2 (&a)[16], int cm) {
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if (e & (1 << K)) continue;
-        if ((e & cm) != cm) continue;
-        const double2 t = a[e];
-        a[e] = a[e | (1 << K)];
-        a[e | (1 << K)] = t;
-    }
-}
-
-template <int K0, int K1>
-__device__ __forceinline__ void reg_swap(double2 (&a)[16]) {
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if ((e & (1 << K0)) && !(e & (1 << K1))) {
-            const int f = e ^ (1 << K0) ^ (1 << K1);
-            const double2 t = a[e];
-            a[e] = a[f];
-            a[f] = t;
-        }
-    }
-}
-
-template <int K0, int K1>
-__device__ __forceinline__ void reg_m2(double2 (&a)[16], const double *__restrict__ c) {
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
-        const int idx[4] = {e, e | (1 << K1), e | (1 << K0), e | (1 << K0) | (1 << K1)};
-        double2 in[4], out[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) in[r] = a[idx[r]];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            double ore = 0.0, oim = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double mr = c[(r * 4 + q) * 2], mi = c[(r * 4 + q) * 2 + 1];
-                ore += mr * in[q].x - mi * in[q].y;
-                oim += mr * in[q].y + mi * in[q].x;
-            }
-            out[r] = make_double2(ore, oim);
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) a[idx[r]] = out[r];
-    }
-}
-
-template <int KB>
-__device__ __forceinline__ void reg_block(double2 (&a)[16], const double *__restrict__ c) {
-    constexpr int D = 1 << KB;
-#pragma unroll
-    for (int hiv = 0; hiv < 16; hiv += D) {
-        double2 in[D];
-#pragma unroll
-        for (int q = 0; q < D; ++q) in[q] = a[hiv + q];
-#pragma unroll
-        for (int r = 0; r < D; ++r) {
-            double ore = 0.0, oim = 0.0;
-#pragma unroll
-            for (int q = 0; q < D; ++q) {
-                const double mr = c[(r * D + q) * 2], mi = c[(r * D + q) * 2 + 1];
-                ore += mr * in[q].x - mi * in[q].y;
-                oim += mr * in[q].y + mi * in[q].x;
-            }
-            a[hiv + r] = make_double2(ore, oim);
-        }
-    }
-}
-
-__device__ __forceinline__ void reg_diag(double2 (&a)[16], const FusedOp &op,
-                                         const double *__restrict__ c) {
-    const double p0r = c[0], p0i = c[1], p1r = c[2], p1i = c[3];
-    const double p2r = c[4], p2i = c[5], p3r = c[6], p3i = c[7];
-    const int k0 = op.k0, k1 = op.k1, np = op.npat, cm = op.cm;
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if ((e & cm) != cm) continue;
-        const int b0 = np > 0 ? (e >> k0) & 1 : 0;
-        const int b1 = np > 1 ? (e >> k1) & 1 : 0;
-        const double pr = b1 ? (b0 ? p3r : p2r) : (b0 ? p1r : p0r);
-        const double pi = b1 ? (b0 ? p3i : p2i) : (b0 ? p1i : p0i);
-        const double2 v = a[e];
-        a[e] = make_double2(v.x * pr - v.y * pi, v.x * pi + v.y * pr);
-    }
-}
-
-template <bool BLOCKS>
-__device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &op,
-                                               const double *__restrict__ coef) {
-    const double *c = coef + op.coef;
-    switch (op.type) {
-    case F_M1:
-        switch (op.k0) {
-        case 0: reg_m1<0>(a, op.cm, c); break;
-        case 1: reg_m1<1>(a, op.cm, c); break;
-        case 2: reg_m1<2>(a, op.cm, c); break;
-        default: reg_m1<3>(a, op.cm, c); break;
-        }
-        break;
-    case F_PERM1:
-        switch (op.k0) {
-        case 0: reg_perm1<0>(a, op.cm); break;
-        case 1: reg_perm1<1>(a, op.cm); break;
-        case 2: reg_perm1<2>(a, op.cm); break;
-        default: reg_perm1<3>(a, op.cm); break;
-        }
-        break;
-    case F_DIAG:
-        reg_diag(a, op, c);
-        break;
-    case F_SWAP: {
-        const int key = op.k0 * 4 + op.k1;
-        switch (key) {
-        case 1: reg_swap<0, 1>(a); break;
-        case 2: reg_swap<0, 2>(a); break;
-        case 3: reg_swap<0, 3>(a); break;
-        case 4: reg_swap<1, 0>(a); break;
-        case 6: reg_swap<1, 2>(a); break;
-        case 7: reg_swap<1, 3>(a); break;
-        case 8: reg_swap<2, 0>(a); break;
-        case 9: reg_swap<2, 1>(a); break;
-        case 11: reg_swap<2, 3>(a); break;
-        case 12: reg_swap<3, 0>(a); break;
-        case 13: reg_swap<3, 1>(a); break;
-        default: reg_swap<3, 2>(a); break;
-        }
-        break;
-    }
-    case F_M2: {
-        if constexpr (!BLOCKS) break;
-        const int key = op.k0 * 4 + op.k1;
-        switch (key) {
-        case 1: reg_m2<0, 1>(a, c); break;
-        case 2: reg_m2<0, 2>(a, c); break;
-        case 3: reg_m2<0, 3>(a, c); break;
-        case 4: reg_m2<1, 0>(a, c); break;
-        case 6: reg_m2<1, 2>(a, c); break;
-        case 7: reg_m2<1, 3>(a, c); break;
-        case 8: reg_m2<2, 0>(a, c); break;
-        case 9: reg_m2<2, 1>(a, c); break;
-        case 11: reg_m2<2, 3>(a, c); break;
-        case 12: reg_m2<3, 0>(a, c); break;
-        case 13: reg_m2<3, 1>(a, c); break;
-        default: reg_m2<3, 2>(a, c); break;
-        }
-        break;
-    }
-    default:
-        if constexpr (BLOCKS) {
-            if (op.type == F_BLOCK3) reg_block<3>(a, c);
-            else reg_block<4>(a, c);
-        }
-        break;
-    }
-}
-
-// Bounded wait on an mbarrier phase.  Returns false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 24); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
+static std::atomic<int> g_fusion_width{11};
+int fusion_width() { return g_fusion_width.load(); }
 
 struct TileCoords {
-    int32_t h4;  // h - 4: width of the dim-2 coordinate inside blockIdx
+    int32_t h;       // window range start (bits h .. h+m-1), h >= 4
+    int32_t hm;      // h + m
+    int32_t ntiles;  // 2^(n-T)
 };
 
-// One CTA = one tile.  blockDim.x = 2^(T-4), dynamic smem = 2^T*16 + 2048.
-template <bool BLOCKS>
+// One CTA per tile.  blockDim.x = 2^(T-4); dynamic smem = 2^T * 16 + 2048.
+// (Measured on B200: more resident CTAs per SM beat a persistent,
+// double-buffered CTA here, because the register-resident gate math needs the
+// warps to hide FP64 latency more than it needs load/compute overlap.)
+// EXT selects the variant that also carries 4x4 and block ops (more registers).
+template <bool EXT>
 __global__ void __launch_bounds__(256, 2)
     k_fused_pass(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                  const FusedRound *__restrict__ rounds, int nrounds,
@@ -270,16 +59,14 @@ __global__ void __launch_bounds__(256, 2)
                  unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    double2 *tile = (double2 *)base;
-    uint64_t *bar = (uint64_t *)(base + (16u << T));
+    const uint32_t tile_bytes = 16u << T;
+    uint64_t *bar = (uint64_t *)(base + tile_bytes);
+    const uint32_t tile_a = smem_u32(base);
     const uint32_t bar_a = smem_u32(bar);
-    const uint32_t tile_a = smem_u32(tile);
     const int tid = threadIdx.x;
-
-    const int32_t bid = (int32_t)blockIdx.x;
-    const int32_t c2 = bid & ((1 << tc.h4) - 1);
-    const int32_t c4 = bid >> tc.h4;
     const int32_t zero = 0;
+    const int tile = blockIdx.x;
+    const int32_t c2 = tile & ((1 << (tc.h - 4)) - 1), c4 = tile >> (tc.h - 4);
 
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1) : "memory");
@@ -287,9 +74,8 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
     if (tid == 0) {
-        const uint32_t bytes = 16u << T;
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
-                     "r"(bytes)
+                     "r"(tile_bytes)
                      : "memory");
         asm volatile(
             "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
@@ -301,31 +87,10 @@ __global__ void __launch_bounds__(256, 2)
         if (tid == 0) atomicOr(flag, kFlagTimeout);
         return;
     }
-
+    const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
+    auto coef_of = [&](const FusedOp &op) { return coef + op.coef; };
     for (int r = 0; r < nrounds; ++r) {
-        const FusedRound &rd = rounds[r];
-        // thread base index: thread bits scattered to the round's lane positions
-        int tbase = 0;
-        for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
-        const int p0 = 1 << rd.rpos[0], p1 = 1 << rd.rpos[1];
-        const int p2 = 1 << rd.rpos[2], p3 = 1 << rd.rpos[3];
-        double2 a[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            const int idx = tbase | ((e & 1) ? p0 : 0) | ((e & 2) ? p1 : 0) |
-                            ((e & 4) ? p2 : 0) | ((e & 8) ? p3 : 0);
-            a[e] = tile[swz(idx)];
-        }
-        for (int o = rd.op_begin; o < rd.op_end; ++o) {
-            const FusedOp op = ops[o];
-            apply_fused_op<BLOCKS>(a, op, coef);
-        }
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            const int idx = tbase | ((e & 1) ? p0 : 0) | ((e & 2) ? p1 : 0) |
-                            ((e & 4) ? p2 : 0) | ((e & 8) ? p3 : 0);
-            tile[swz(idx)] = a[e];
-        }
+        run_round<EXT>(tile_a, rounds[r], ops, coef_of, tile_base, tc.h, tid);
         __syncthreads();
     }
     // Make the generic-proxy writes visible to the TMA engine, then store.
@@ -384,32 +149,18 @@ static int make_tile_map(CUtensorMap *map, void *d, int n, int h, int m) {
 // ---------------------------------------------------------------------------
 // Host: planner
 // ---------------------------------------------------------------------------
-struct PlannedRound {
-    int rpos[4];
-    std::vector<int> ops;  // indices into the pass op list
-    bool block = false;
-};
-
-struct PlannedPass {
-    int h = 4;
-    std::vector<int> gates;  // indices into the circuit op list (in order)
-    std::vector<PlannedRound> rounds;
-};
-
-struct PlanStep {  // either a fused pass or a standalone gate
-    bool fused = false;
-    int gate = -1;
-    PlannedPass pass;
-};
-
 static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 
-static uint64_t window_mask(int h, int m) {
-    return 0xFull | (((1ull << m) - 1) << h);
+// Bits an op mixes or permutes (they must sit in the register set R).
+static uint64_t reg_bits(const GateOp &o) {
+    switch (o.type) {
+    case OP_M1:
+    case OP_PERM1: return 1ull << o.t;
+    case OP_SWAP:
+    case OP_M2: return (1ull << o.b0) | (1ull << o.b1);
+    default: return 0;  // diagonal
+    }
 }
-
-// Local position of global bit b inside the window [0,4) U [h, h+m).
-static inline int local_pos(int b, int h) { return b < 4 ? b : 4 + (b - h); }
 
 static int choose_lanes(const int rpos[4], int T, int *lane) {
     // Thread-index bits go to the tile positions outside R.  The first three
@@ -454,22 +205,22 @@ static void pad_rpos(std::vector<int> &R, int T) {
     }
 }
 
-static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
-                                  const std::vector<int> &order_idx) {
+std::vector<PlanStep> plan_circuit(const std::vector<GateOp> &gops, int n, int T) {
     const int m = T - 4;
     std::vector<PlanStep> steps;
-    const int G = (int)order_idx.size();
+    const int G = (int)gops.size();
+    const uint64_t all = (1ull << n) - 1;
     std::vector<char> done(G, 0);
-    std::vector<uint64_t> bits(G);
-    std::vector<int> nb(G);
+    std::vector<uint64_t> bits(G), rbits(G);
+    std::vector<char> fusable(G);
     for (int i = 0; i < G; ++i) {
-        bits[i] = op_bits(gops[order_idx[i]]);
-        nb[i] = popc(bits[i]);
+        bits[i] = op_bits(gops[i]);
+        rbits[i] = reg_bits(gops[i]);
+        fusable[i] = !gops[i].renorm && popc(rbits[i]) <= 4;
     }
     int remaining = G, first = 0;
     while (remaining > 0) {
         while (first < G && done[first]) ++first;
-        // Best window.
         int best_h = -1, best_cnt = 0;
         for (int h = 4; h + m <= n; ++h) {
             const uint64_t W = window_mask(h, m);
@@ -477,13 +228,12 @@ static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
             int cnt = 0;
             for (int i = first; i < G; ++i) {
                 if (done[i]) continue;
-                if ((bits[i] & ~W) == 0 && (bits[i] & blocked) == 0 &&
-                    !gops[order_idx[i]].renorm && nb[i] <= 4) {
+                if (fusable[i] && (rbits[i] & ~W) == 0 && (bits[i] & blocked) == 0) {
                     ++cnt;
                 } else {
                     // A renormalising gate is a barrier for every bit.
-                    blocked |= gops[order_idx[i]].renorm ? ~0ull : bits[i];
-                    if ((blocked & ((1ull << n) - 1)) == ((1ull << n) - 1)) break;
+                    blocked |= gops[i].renorm ? all : bits[i];
+                    if ((blocked & all) == all) break;
                 }
             }
             if (cnt > best_cnt) {
@@ -494,7 +244,7 @@ static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
         if (best_cnt == 0) {
             PlanStep st;
             st.fused = false;
-            st.gate = order_idx[first];
+            st.gate = first;
             steps.push_back(st);
             done[first] = 1;
             --remaining;
@@ -507,25 +257,27 @@ static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
         uint64_t blocked = 0;
         for (int i = first; i < G; ++i) {
             if (done[i]) continue;
-            if ((bits[i] & ~W) == 0 && (bits[i] & blocked) == 0 && !gops[order_idx[i]].renorm &&
-                nb[i] <= 4) {
-                st.pass.gates.push_back(order_idx[i]);
+            if (fusable[i] && (rbits[i] & ~W) == 0 && (bits[i] & blocked) == 0) {
+                st.pass.gates.push_back(i);
                 done[i] = 1;
                 --remaining;
             } else {
-                blocked |= gops[order_idx[i]].renorm ? ~0ull : bits[i];
+                blocked |= gops[i].renorm ? all : bits[i];
+                if ((blocked & all) == all) break;
             }
         }
-        // Rounds.
+        // Rounds: greedy, in order; an op joins the round if it is not blocked by
+        // an earlier unscheduled op sharing a bit and its register bits fit R.
         const int P = (int)st.pass.gates.size();
         std::vector<char> sched(P, 0);
-        std::vector<uint64_t> lb(P);
+        std::vector<uint64_t> lreg(P), gall(P);
         for (int k = 0; k < P; ++k) {
-            const uint64_t gb = op_bits(gops[st.pass.gates[k]]);
+            const int i = st.pass.gates[k];
             uint64_t l = 0;
             for (int b = 0; b < n; ++b)
-                if (gb >> b & 1) l |= 1ull << local_pos(b, best_h);
-            lb[k] = l;
+                if (rbits[i] >> b & 1) l |= 1ull << local_pos(b, best_h);
+            lreg[k] = l;
+            gall[k] = bits[i];
         }
         int left = P;
         while (left > 0) {
@@ -533,13 +285,13 @@ static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
             uint64_t R = 0, blk = 0;
             for (int k = 0; k < P; ++k) {
                 if (sched[k]) continue;
-                if ((lb[k] & blk) == 0 && popc(R | lb[k]) <= 4) {
-                    R |= lb[k];
+                if ((gall[k] & blk) == 0 && popc(R | lreg[k]) <= 4) {
+                    R |= lreg[k];
                     rd.ops.push_back(k);
                     sched[k] = 1;
                     --left;
                 } else {
-                    blk |= lb[k];
+                    blk |= gall[k];
                 }
             }
             std::vector<int> Rv;
@@ -554,11 +306,21 @@ static std::vector<PlanStep> plan(const std::vector<GateOp> &gops, int n, int T,
     return steps;
 }
 
-// Encode one gate (already part of a round with register positions rpos) as a
-// register op.  lbit(b) maps a global bit to its register index.
-static void encode_op(const GateOp &g, int h, const int rpos[4], std::vector<FusedOp> &fops,
-                      std::vector<double> &coef) {
+void fill_round(FusedRound &fr, const int rpos[4], int T, int h) {
+    for (int e = 0; e < 16; ++e) {
+        int off = 0;
+        for (int k = 0; k < 4; ++k)
+            if (e >> k & 1) off |= 1 << rpos[k];
+        fr.eoff[e] = swz(off) << 4;
+    }
+    for (int k = 0; k < 4; ++k) fr.gpos[k] = 1ull << global_pos(rpos[k], h);
+    fr.nlane = choose_lanes(rpos, T, fr.lane);
+}
+
+void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<FusedOp> &fops,
+               std::vector<double> &coef) {
     auto reg = [&](int b) {
+        if (!(b < 4 || (b >= h && b < h + m))) return -1;  // outside the window
         const int lp = local_pos(b, h);
         for (int k = 0; k < 4; ++k)
             if (rpos[k] == lp) return k;
@@ -566,28 +328,43 @@ static void encode_op(const GateOp &g, int h, const int rpos[4], std::vector<Fus
     };
     FusedOp f{};
     f.coef = (int)coef.size();
+    f.pb0 = f.pb1 = -1;
+    f.param = -1;
+    f.coef_alt = -1;
     switch (g.type) {
     case OP_M1:
-    case OP_PERM1:
-        f.type = g.type == OP_M1 ? F_M1 : F_PERM1;
+    case OP_PERM1: {
         f.k0 = reg(g.t);
         f.cm = 0;
-        for (int c = 0; c < g.nctrl; ++c) f.cm |= 1 << reg(g.ctrl[c]);
-        if (g.type == OP_M1) coef.insert(coef.end(), g.m, g.m + 8);
+        f.gmask = 0;
+        for (int c = 0; c < g.nctrl; ++c) {
+            const int k = reg(g.ctrl[c]);
+            if (k >= 0) f.cm |= 1 << k;
+            else f.gmask |= 1ull << g.ctrl[c];
+        }
+        if (g.type == OP_M1) {
+            f.type = f.cm ? F_M1C : F_M1;
+            coef.insert(coef.end(), g.m, g.m + 8);
+        } else {
+            f.type = f.cm ? F_XC : F_X;
+            coef.insert(coef.end(), 8, 0.0);
+        }
         break;
+    }
     case OP_DIAG:
         f.type = F_DIAG;
         f.npat = g.npat;
-        f.k0 = g.npat > 0 ? reg(g.pat[0]) : 0;
-        f.k1 = g.npat > 1 ? reg(g.pat[1]) : 0;
-        f.cm = 0;
-        for (int c = 0; c < g.nfix; ++c) f.cm |= 1 << reg(g.fix[c]);
+        f.pb0 = g.npat > 0 ? g.pat[0] : -1;
+        f.pb1 = g.npat > 1 ? g.pat[1] : -1;
+        f.fixmask = 0;
+        for (int c = 0; c < g.nfix; ++c) f.fixmask |= 1ull << g.fix[c];
         coef.insert(coef.end(), g.m, g.m + 8);
         break;
     case OP_SWAP:
         f.type = F_SWAP;
         f.k0 = reg(g.b0);
         f.k1 = reg(g.b1);
+        coef.insert(coef.end(), 8, 0.0);
         break;
     case OP_M2:
         f.type = F_M2;
@@ -602,8 +379,72 @@ static void encode_op(const GateOp &g, int h, const int rpos[4], std::vector<Fus
 struct PassLaunch {
     int h;
     int round_begin, nrounds;
-    bool extended;  // holds 4x4 ops: needs the extended kernel variant
+    bool extended;  // holds 4x4 / block ops: needs the extended kernel variant
 };
+
+static size_t fused_smem(int T) { return (16u << T) + 2048; }
+
+static int fused_grid(int T, int ntiles, bool extended) {
+    (void)T;
+    (void)extended;
+    return ntiles;
+}
+
+static int set_smem_attrs() {
+    static bool done = false;
+    if (done) return LQ_OK;
+    const int mx = (int)fused_smem(kMaxT);
+    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    done = true;
+    return LQ_OK;
+}
+
+static int launch_pass(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
+                       const FusedOp *d_ops, const double *d_coef, bool extended) {
+    const int n = s->n;
+    const int m = T - 4;
+    CUtensorMap map;
+    LQ_TRY(make_tile_map(&map, s->d, n, h, m));
+    const int ntiles = 1 << (n - T);
+    TileCoords tc{h, h + m, ntiles};
+    const int grid = fused_grid(T, ntiles, extended);
+    const size_t smem = fused_smem(T);
+    prof_begin(s->stream, kProfFused);
+    if (extended)
+        k_fused_pass<true><<<grid, 1 << (T - 4), smem, s->stream>>>(map, T, tc, d_rounds, nrounds,
+                                                                    d_ops, d_coef, s->d_flag);
+    else
+        k_fused_pass<false><<<grid, 1 << (T - 4), smem, s->stream>>>(
+            map, T, tc, d_rounds, nrounds, d_ops, d_coef, s->d_flag);
+    prof_end(s->stream, kProfFused);
+    LQ_CUDA_TRY(cudaGetLastError());
+    return LQ_OK;
+}
+
+// Build the device program of every fused pass of `steps`.
+static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<GateOp> &gops,
+                         int T, std::vector<FusedRound> &rounds, std::vector<FusedOp> &fops,
+                         std::vector<double> &coef, std::vector<PassLaunch> &launches) {
+    for (auto &st : steps) {
+        if (!st.fused) continue;
+        PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), false};
+        for (auto &rd : st.pass.rounds) {
+            FusedRound fr{};
+            fill_round(fr, rd.rpos, T, st.pass.h);
+            fr.op_begin = (int)fops.size();
+            for (int k : rd.ops) {
+                encode_op(gops[st.pass.gates[k]], st.pass.h, T - 4, rd.rpos, fops, coef);
+                if (fops.back().type == F_M2) pl.extended = true;
+            }
+            fr.op_end = (int)fops.size();
+            rounds.push_back(fr);
+        }
+        launches.push_back(pl);
+    }
+}
 
 int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *theta,
                        int ntheta, int mode) {
@@ -623,34 +464,13 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
         }
         return LQ_OK;
     }
-    const int T = std::min(kMaxT, n);
-    const int m = T - 4;
-    std::vector<int> order(nops);
-    for (int i = 0; i < nops; ++i) order[i] = i;
-    std::vector<PlanStep> steps = plan(gops, n, T, order);
-
-    // Encode every fused pass into one device program.
+    const int T = std::min(fusion_width(), n);
+    std::vector<PlanStep> steps = plan_circuit(gops, n, T);
     std::vector<FusedRound> rounds;
     std::vector<FusedOp> fops;
     std::vector<double> coef;
     std::vector<PassLaunch> launches;
-    for (auto &st : steps) {
-        if (!st.fused) continue;
-        PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), false};
-        for (auto &rd : st.pass.rounds) {
-            FusedRound fr{};
-            for (int k = 0; k < 4; ++k) fr.rpos[k] = rd.rpos[k];
-            fr.nlane = choose_lanes(rd.rpos, T, fr.lane);
-            fr.op_begin = (int)fops.size();
-            for (int k : rd.ops) {
-                encode_op(gops[st.pass.gates[k]], st.pass.h, rd.rpos, fops, coef);
-                if (fops.back().type == F_M2) pl.extended = true;
-            }
-            fr.op_end = (int)fops.size();
-            rounds.push_back(fr);
-        }
-        launches.push_back(pl);
-    }
+    encode_steps(steps, gops, T, rounds, fops, coef, launches);
     const size_t rb = rounds.size() * sizeof(FusedRound);
     const size_t ob = fops.size() * sizeof(FusedOp);
     const size_t cb = coef.size() * sizeof(double);
@@ -665,18 +485,8 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
     if (rb) LQ_CUDA_TRY(cudaMemcpy(d_rounds, rounds.data(), rb, cudaMemcpyHostToDevice));
     if (ob) LQ_CUDA_TRY(cudaMemcpy(d_ops, fops.data(), ob, cudaMemcpyHostToDevice));
     if (cb) LQ_CUDA_TRY(cudaMemcpy(d_coef, coef.data(), cb, cudaMemcpyHostToDevice));
+    LQ_TRY(set_smem_attrs());
 
-    static bool attr_set = false;
-    const size_t smem = (16u << T) + 2048;
-    if (!attr_set) {
-        LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (16 << kMaxT) + 2048));
-        LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (16 << kMaxT) + 2048));
-        attr_set = true;
-    }
     size_t li = 0;
     for (auto &st : steps) {
         if (!st.fused) {
@@ -685,49 +495,11 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
             continue;
         }
         const PassLaunch &pl = launches[li++];
-        CUtensorMap map;
-        LQ_TRY(make_tile_map(&map, s->d, n, pl.h, m));
-        TileCoords tc{pl.h - 4};
-        const unsigned grid = 1u << (n - T);
-        prof_begin(s->stream, kProfFused);
-        if (pl.extended)
-            k_fused_pass<true><<<grid, 1 << (T - 4), smem, s->stream>>>(
-                map, T, tc, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef, s->d_flag);
-        else
-            k_fused_pass<false><<<grid, 1 << (T - 4), smem, s->stream>>>(
-                map, T, tc, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef, s->d_flag);
-        prof_end(s->stream, kProfFused);
-        LQ_CUDA_TRY(cudaGetLastError());
+        LQ_TRY(launch_pass(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef,
+                           pl.extended));
         s->last_launches += 1;
         s->last_passes += 1;
     }
-    return LQ_OK;
-}
-
-static int launch_single_round(lq_state *s, int h, const FusedRound &fr, const FusedOp &fo,
-                               const std::vector<double> &coef) {
-    const int n = s->n;
-    const int T = std::min(kMaxT, n);
-    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t cb = coef.size() * sizeof(double);
-    LQ_TRY(ensure_prog(s, al(sizeof(FusedRound)) + al(sizeof(FusedOp)) + al(cb) + 256));
-    char *dp = (char *)s->d_prog;
-    FusedRound *d_rounds = (FusedRound *)dp;
-    FusedOp *d_ops = (FusedOp *)(dp + al(sizeof(FusedRound)));
-    double *d_coef = (double *)(dp + al(sizeof(FusedRound)) + al(sizeof(FusedOp)));
-    LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    LQ_CUDA_TRY(cudaMemcpy(d_rounds, &fr, sizeof(FusedRound), cudaMemcpyHostToDevice));
-    LQ_CUDA_TRY(cudaMemcpy(d_ops, &fo, sizeof(FusedOp), cudaMemcpyHostToDevice));
-    LQ_CUDA_TRY(cudaMemcpy(d_coef, coef.data(), cb, cudaMemcpyHostToDevice));
-    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (16 << kMaxT) + 2048));
-    CUtensorMap map;
-    LQ_TRY(make_tile_map(&map, s->d, n, h, T - 4));
-    TileCoords tc{h - 4};
-    k_fused_pass<true><<<1u << (n - T), 1 << (T - 4), (16u << T) + 2048, s->stream>>>(
-        map, T, tc, d_rounds, 1, d_ops, d_coef, s->d_flag);
-    LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
 }
 
@@ -736,7 +508,7 @@ int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m) {
     if (k == 1) return lq_apply_matrix1(s, qubits[0], m);
     if (k == 2) return lq_apply_matrix2(s, qubits[0], qubits[1], m);
     if (s->dtype != LQ_C128)
-        return set_error(LQ_ERR_UNSUPPORTED, "block gates on complex64 states use lq_tc_*");
+        return set_error(LQ_ERR_UNSUPPORTED, "block gates need a complex128 state");
     if (n < 5) return set_error(LQ_ERR_UNSUPPORTED, "block gates need at least 5 qubits");
     const int T = std::min(kMaxT, n), mm = T - 4;
     int lo = n, hi = -1;
@@ -757,16 +529,30 @@ int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m) {
     std::vector<int> Rv;
     for (int j = 0; j < k; ++j) Rv.push_back(local_pos(n - 1 - qubits[k - 1 - j], h));
     pad_rpos(Rv, T);
+    int rpos[4];
+    for (int j = 0; j < 4; ++j) rpos[j] = Rv[j];
     FusedRound fr{};
-    for (int j = 0; j < 4; ++j) fr.rpos[j] = Rv[j];
-    fr.nlane = choose_lanes(fr.rpos, T, fr.lane);
+    fill_round(fr, rpos, T, h);
     fr.op_begin = 0;
     fr.op_end = 1;
     FusedOp fo{};
     fo.type = k == 3 ? F_BLOCK3 : F_BLOCK4;
+    fo.pb0 = fo.pb1 = -1;
+    fo.param = fo.coef_alt = -1;
     fo.coef = 0;
-    std::vector<double> coef(m, m + 2 * (1 << k) * (1 << k));
-    return launch_single_round(s, h, fr, fo, coef);
+    const size_t cb = sizeof(double) * 2 * (1 << k) * (1 << k);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    LQ_TRY(ensure_prog(s, al(sizeof(FusedRound)) + al(sizeof(FusedOp)) + al(cb) + 256));
+    char *dp = (char *)s->d_prog;
+    FusedRound *d_rounds = (FusedRound *)dp;
+    FusedOp *d_ops = (FusedOp *)(dp + al(sizeof(FusedRound)));
+    double *d_coef = (double *)(dp + al(sizeof(FusedRound)) + al(sizeof(FusedOp)));
+    LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    LQ_CUDA_TRY(cudaMemcpy(d_rounds, &fr, sizeof(FusedRound), cudaMemcpyHostToDevice));
+    LQ_CUDA_TRY(cudaMemcpy(d_ops, &fo, sizeof(FusedOp), cudaMemcpyHostToDevice));
+    LQ_CUDA_TRY(cudaMemcpy(d_coef, m, cb, cudaMemcpyHostToDevice));
+    LQ_TRY(set_smem_attrs());
+    return launch_pass(s, T, h, d_rounds, 1, d_ops, d_coef, true);
 }
 
 }  // namespace lq
@@ -789,6 +575,19 @@ int lq_apply_circuit(lq_state *s, int circuit_qubits, const lq_gate *ops, int no
     return apply_circuit_impl(s, ops, nops, theta, ntheta, mode);
 }
 
+int lq_set_fusion_width(int tile_bits) {
+    if (tile_bits < 5 || tile_bits > kMaxT)
+        return set_error(LQ_ERR_INVALID_ARG, "fusion width must be 5..%d", kMaxT);
+    g_fusion_width.store(tile_bits);
+    return LQ_OK;
+}
+
+int lq_get_fusion_width(int *tile_bits) {
+    if (!tile_bits) return set_error(LQ_ERR_INVALID_ARG, "null output");
+    *tile_bits = fusion_width();
+    return LQ_OK;
+}
+
 int lq_apply_block(lq_state *s, int k, const int *qubits, const double *m) {
     LQ_TRY(check_state(s));
     if (k < 1 || k > 4 || !qubits || !m)
@@ -801,24 +600,33 @@ int lq_apply_block(lq_state *s, int k, const int *qubits, const double *m) {
     return apply_block_impl(s, k, qubits, m);
 }
 
-int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, int *rounds,
-                    int *standalone) {
+static int plan_for(int num_qubits, const lq_gate *ops, int nops, const double *theta,
+                    int ntheta, std::vector<GateOp> &gops, std::vector<PlanStep> &steps,
+                    int &T) {
     if (nops < 0 || (nops > 0 && !ops)) return set_error(LQ_ERR_INVALID_ARG, "bad op list");
     if (num_qubits < 5 || num_qubits > 36)
         return set_error(LQ_ERR_UNSUPPORTED, "fused planning needs 5..36 qubits");
-    std::vector<GateOp> gops(nops);
+    gops.resize(nops);
+    static const double zero_theta[1] = {0.0};
     for (int i = 0; i < nops; ++i) {
-        LQ_TRY(validate_gate(&ops[i], num_qubits, 1 << 30));
-        static const double zero_theta[1] = {0.0};
-        // Angles do not change the plan; bound parameters read theta[0].
         lq_gate g = ops[i];
-        for (int k = 0; k < 3; ++k) g.param[k] = -1;
-        LQ_TRY(make_gate_op(&g, zero_theta, num_qubits, &gops[i]));
+        if (!theta) {  // angles do not change the plan: unbind parameters
+            for (int k = 0; k < 3; ++k) g.param[k] = -1;
+        }
+        LQ_TRY(validate_gate(&g, num_qubits, theta ? ntheta : 1 << 30));
+        LQ_TRY(make_gate_op(&g, theta ? theta : zero_theta, num_qubits, &gops[i]));
     }
-    const int T = std::min(kMaxT, num_qubits);
-    std::vector<int> order(nops);
-    for (int i = 0; i < nops; ++i) order[i] = i;
-    std::vector<PlanStep> steps = plan(gops, num_qubits, T, order);
+    T = std::min(fusion_width(), num_qubits);
+    steps = plan_circuit(gops, num_qubits, T);
+    return LQ_OK;
+}
+
+int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, int *rounds,
+                    int *standalone) {
+    std::vector<GateOp> gops;
+    std::vector<PlanStep> steps;
+    int T;
+    LQ_TRY(plan_for(num_qubits, ops, nops, nullptr, 0, gops, steps, T));
     int p = 0, r = 0, s1 = 0;
     for (auto &st : steps) {
         if (st.fused) {
@@ -831,6 +639,49 @@ int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, i
     if (passes) *passes = p;
     if (rounds) *rounds = r;
     if (standalone) *standalone = s1;
+    return LQ_OK;
+}
+
+int lq_plan_dump(int num_qubits, const lq_gate *ops, int nops, const double *theta, int ntheta,
+                 void *buf, size_t cap, size_t *used) {
+    // Layout (little endian): int32 counts[5] = {nsteps, nrounds, nops, ncoef, T},
+    // then nsteps x int32[5] {fused, gate, h, round_begin, nrounds},
+    // nrounds x FusedRound, nops x FusedOp, ncoef x double.
+    std::vector<GateOp> gops;
+    std::vector<PlanStep> steps;
+    int T;
+    LQ_TRY(plan_for(num_qubits, ops, nops, theta, ntheta, gops, steps, T));
+    std::vector<FusedRound> rounds;
+    std::vector<FusedOp> fops;
+    std::vector<double> coef;
+    std::vector<PassLaunch> launches;
+    encode_steps(steps, gops, T, rounds, fops, coef, launches);
+    std::vector<int32_t> st_rec;
+    size_t li = 0;
+    for (auto &st : steps) {
+        if (!st.fused) {
+            st_rec.insert(st_rec.end(), {0, st.gate, 0, 0, 0});
+        } else {
+            const PassLaunch &pl = launches[li++];
+            st_rec.insert(st_rec.end(), {1, -1, pl.h, pl.round_begin, pl.nrounds});
+        }
+    }
+    const int32_t counts[5] = {(int32_t)steps.size(), (int32_t)rounds.size(),
+                               (int32_t)fops.size(), (int32_t)coef.size(), T};
+    const size_t need = sizeof(counts) + st_rec.size() * 4 + rounds.size() * sizeof(FusedRound) +
+                        fops.size() * sizeof(FusedOp) + coef.size() * 8;
+    if (used) *used = need;
+    if (!buf || cap < need) return set_error(LQ_ERR_INVALID_ARG, "buffer too small (%zu)", need);
+    char *p = (char *)buf;
+    memcpy(p, counts, sizeof(counts));
+    p += sizeof(counts);
+    memcpy(p, st_rec.data(), st_rec.size() * 4);
+    p += st_rec.size() * 4;
+    memcpy(p, rounds.data(), rounds.size() * sizeof(FusedRound));
+    p += rounds.size() * sizeof(FusedRound);
+    memcpy(p, fops.data(), fops.size() * sizeof(FusedOp));
+    p += fops.size() * sizeof(FusedOp);
+    memcpy(p, coef.data(), coef.size() * 8);
     return LQ_OK;
 }
 

@@ -1,0 +1,328 @@
+// Register-level gate ops shared by the fused pass kernel (fused.cu) and the
+// batched parameter-shift engine (batch.cu).
+//
+// A thread holds 16 amplitudes that differ only in four tile bits R (its
+// "register bits"); each op below acts on those registers.  Ops are encoded
+// by the host planner (fused.cu) as FusedOp records.
+#pragma once
+
+#include <cstdint>
+
+#include "lq_internal.h"
+
+namespace lq {
+
+enum FusedOpType {
+    F_M1 = 0,     // 2x2 on reg bit k0
+    F_M1C = 1,    // 2x2 on reg bit k0 where the register bits cm are all 1
+    F_X = 2,      // X on reg bit k0
+    F_XC = 3,     // X on reg bit k0 where the register bits cm are all 1
+    F_DIAG = 4,   // amplitude *= ph[pattern] where the global index bits fixmask are all 1;
+                  // pattern = index bits pb0 (lsb), pb1
+    F_SWAP = 5,   // swap reg bits k0, k1
+    F_M2 = 6,     // 4x4, index = bit(k0)<<1 | bit(k1)
+    F_BLOCK3 = 7, // 8x8 on reg bits 0..2 (matrix bit j <-> reg bit j)
+    F_BLOCK4 = 8  // 16x16 on reg bits 0..3
+};
+
+struct FusedOp {
+    int32_t type;
+    int32_t k0, k1, cm;
+    uint64_t gmask;    // thread-level condition: global index bits outside R, all must be 1
+    uint64_t fixmask;  // F_DIAG element condition (any global bits)
+    int32_t pb0, pb1;  // F_DIAG pattern bit positions (global)
+    int32_t npat;
+    int32_t coef;      // offset of the coefficients in the coefficient array (doubles)
+    int32_t param;     // batched engine: parameter the op's angle is bound to (-1: none)
+    int32_t coef_alt;  // batched engine: offset of the (+shift, -shift) coefficient pair
+};
+
+struct FusedRound {
+    int32_t eoff[16];  // swizzled byte offset of register element e relative to the thread base
+    uint64_t gpos[4];  // global index mask of register bits 0..3
+    int32_t lane[12];  // tile-local positions of the thread-index bits, in order
+    int32_t nlane;
+    int32_t op_begin, op_end;
+    int32_t pad;
+};
+
+constexpr int kMaxT = 12;
+
+// 128-byte TMA swizzle of a tile-local amplitude index: the 16-byte chunk
+// (index bits 0-2) is XORed with the 128-byte row (index bits 3-5).
+__host__ __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ double2 cmul_add4(double ar, double ai, double2 x, double br,
+                                             double bi, double2 y) {
+    // (a * x + b * y) with one multiply and three FMAs per real output.
+    double2 o;
+    o.x = fma(-bi, y.y, fma(br, y.x, fma(-ai, x.y, ar * x.x)));
+    o.y = fma(bi, y.x, fma(br, y.y, fma(ai, x.x, ar * x.y)));
+    return o;
+}
+
+template <int K, bool CM>
+__device__ __forceinline__ void reg_m1(double2 (&a)[16], int cm, const double (&c)[8]) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if (e & (1 << K)) continue;
+        if (CM && (e & cm) != cm) continue;
+        const double2 a0 = a[e], a1 = a[e | (1 << K)];
+        a[e] = cmul_add4(c[0], c[1], a0, c[2], c[3], a1);
+        a[e | (1 << K)] = cmul_add4(c[4], c[5], a0, c[6], c[7], a1);
+    }
+}
+
+template <int K, bool CM>
+__device__ __forceinline__ void reg_x(double2 (&a)[16], int cm) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if (e & (1 << K)) continue;
+        if (CM && (e & cm) != cm) continue;
+        const double2 t = a[e];
+        a[e] = a[e | (1 << K)];
+        a[e | (1 << K)] = t;
+    }
+}
+
+template <int K0, int K1>
+__device__ __forceinline__ void reg_swap(double2 (&a)[16]) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if ((e & (1 << K0)) && !(e & (1 << K1))) {
+            const int f = e ^ (1 << K0) ^ (1 << K1);
+            const double2 t = a[e];
+            a[e] = a[f];
+            a[f] = t;
+        }
+    }
+}
+
+template <int K0, int K1>
+__device__ __forceinline__ void reg_m2(double2 (&a)[16], const double *__restrict__ c) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
+        const int idx[4] = {e, e | (1 << K1), e | (1 << K0), e | (1 << K0) | (1 << K1)};
+        double2 in[4], out[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) in[r] = a[idx[r]];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            double ore = 0.0, oim = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double mr = c[(r * 4 + q) * 2], mi = c[(r * 4 + q) * 2 + 1];
+                ore = fma(-mi, in[q].y, fma(mr, in[q].x, ore));
+                oim = fma(mi, in[q].x, fma(mr, in[q].y, oim));
+            }
+            out[r] = make_double2(ore, oim);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) a[idx[r]] = out[r];
+    }
+}
+
+template <int KB>
+__device__ __forceinline__ void reg_block(double2 (&a)[16], const double *__restrict__ c) {
+    constexpr int D = 1 << KB;
+#pragma unroll
+    for (int hiv = 0; hiv < 16; hiv += D) {
+        double2 in[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) in[q] = a[hiv + q];
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            double ore = 0.0, oim = 0.0;
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                const double mr = c[(r * D + q) * 2], mi = c[(r * D + q) * 2 + 1];
+                ore = fma(-mi, in[q].y, fma(mr, in[q].x, ore));
+                oim = fma(mi, in[q].x, fma(mr, in[q].y, oim));
+            }
+            a[hiv + r] = make_double2(ore, oim);
+        }
+    }
+}
+
+// Diagonal op: every bit it reads comes from the element's global index
+// gbase | goff(e), goff(e) = OR of gpos[k] over the set bits k of e.
+__device__ __forceinline__ void reg_diag(double2 (&a)[16], const FusedOp &op,
+                                         const double (&c)[8], uint64_t gbase,
+                                         const uint64_t *__restrict__ gpp) {
+    const uint64_t gp[4] = {gpp[0], gpp[1], gpp[2], gpp[3]};
+    const uint64_t fm = op.fixmask;
+    const int pb0 = op.pb0 < 0 ? 0 : op.pb0, pb1 = op.pb1 < 0 ? 0 : op.pb1;
+    const uint64_t use0 = op.npat > 0 ? 1ull : 0ull, use1 = op.npat > 1 ? 1ull : 0ull;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const uint64_t gi = gbase | ((e & 1) ? gp[0] : 0ull) | ((e & 2) ? gp[1] : 0ull) |
+                            ((e & 4) ? gp[2] : 0ull) | ((e & 8) ? gp[3] : 0ull);
+        if ((gi & fm) != fm) continue;
+        const int b0 = (int)((gi >> pb0) & use0), b1 = (int)((gi >> pb1) & use1);
+        const double pr = b1 ? (b0 ? c[6] : c[4]) : (b0 ? c[2] : c[0]);
+        const double pi = b1 ? (b0 ? c[7] : c[5]) : (b0 ? c[3] : c[1]);
+        const double2 v = a[e];
+        a[e] = make_double2(fma(-v.y, pi, v.x * pr), fma(v.x, pi, v.y * pr));
+    }
+}
+
+// Apply one op.  c8 holds the op's first eight coefficients (prefetched by the
+// caller); cfull points at all of them (4x4 and block ops read more).
+template <bool EXT>
+__device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &op,
+                                               const double (&c8)[8],
+                                               const double *__restrict__ cfull, uint64_t gbase,
+                                               const uint64_t *__restrict__ gp) {
+    if ((gbase & op.gmask) != op.gmask) return;  // a control outside R is 0
+    switch (op.type) {
+    case F_M1:
+        switch (op.k0) {
+        case 0: reg_m1<0, false>(a, 0, c8); break;
+        case 1: reg_m1<1, false>(a, 0, c8); break;
+        case 2: reg_m1<2, false>(a, 0, c8); break;
+        default: reg_m1<3, false>(a, 0, c8); break;
+        }
+        break;
+    case F_M1C:
+        switch (op.k0) {
+        case 0: reg_m1<0, true>(a, op.cm, c8); break;
+        case 1: reg_m1<1, true>(a, op.cm, c8); break;
+        case 2: reg_m1<2, true>(a, op.cm, c8); break;
+        default: reg_m1<3, true>(a, op.cm, c8); break;
+        }
+        break;
+    case F_X:
+        switch (op.k0) {
+        case 0: reg_x<0, false>(a, 0); break;
+        case 1: reg_x<1, false>(a, 0); break;
+        case 2: reg_x<2, false>(a, 0); break;
+        default: reg_x<3, false>(a, 0); break;
+        }
+        break;
+    case F_XC:
+        switch (op.k0) {
+        case 0: reg_x<0, true>(a, op.cm); break;
+        case 1: reg_x<1, true>(a, op.cm); break;
+        case 2: reg_x<2, true>(a, op.cm); break;
+        default: reg_x<3, true>(a, op.cm); break;
+        }
+        break;
+    case F_DIAG:
+        reg_diag(a, op, c8, gbase, gp);
+        break;
+    case F_SWAP: {
+        const int key = op.k0 * 4 + op.k1;
+        switch (key) {
+        case 1: reg_swap<0, 1>(a); break;
+        case 2: reg_swap<0, 2>(a); break;
+        case 3: reg_swap<0, 3>(a); break;
+        case 4: reg_swap<1, 0>(a); break;
+        case 6: reg_swap<1, 2>(a); break;
+        case 7: reg_swap<1, 3>(a); break;
+        case 8: reg_swap<2, 0>(a); break;
+        case 9: reg_swap<2, 1>(a); break;
+        case 11: reg_swap<2, 3>(a); break;
+        case 12: reg_swap<3, 0>(a); break;
+        case 13: reg_swap<3, 1>(a); break;
+        default: reg_swap<3, 2>(a); break;
+        }
+        break;
+    }
+    default:
+        if constexpr (EXT) {
+            if (op.type == F_M2) {
+                const int key = op.k0 * 4 + op.k1;
+                switch (key) {
+                case 1: reg_m2<0, 1>(a, cfull); break;
+                case 2: reg_m2<0, 2>(a, cfull); break;
+                case 3: reg_m2<0, 3>(a, cfull); break;
+                case 4: reg_m2<1, 0>(a, cfull); break;
+                case 6: reg_m2<1, 2>(a, cfull); break;
+                case 7: reg_m2<1, 3>(a, cfull); break;
+                case 8: reg_m2<2, 0>(a, cfull); break;
+                case 9: reg_m2<2, 1>(a, cfull); break;
+                case 11: reg_m2<2, 3>(a, cfull); break;
+                case 12: reg_m2<3, 0>(a, cfull); break;
+                case 13: reg_m2<3, 1>(a, cfull); break;
+                default: reg_m2<3, 2>(a, cfull); break;
+                }
+            } else if (op.type == F_BLOCK3) {
+                reg_block<3>(a, cfull);
+            } else {
+                reg_block<4>(a, cfull);
+            }
+        }
+        break;
+    }
+}
+
+// One round on a tile in shared memory: gather 16 registers per thread, run
+// the round's ops (op descriptors and their first coefficients prefetched one
+// op ahead), scatter back.  coef_of(op) returns the op's coefficient pointer.
+template <bool EXT, class CoefOf>
+__device__ __forceinline__ void run_round(uint32_t tile_a, const FusedRound &rd,
+                                          const FusedOp *__restrict__ ops, CoefOf coef_of,
+                                          uint64_t tile_base, int h, int tid) {
+    int tbase = 0;
+    for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
+    // swizzled byte offset of the thread base (XOR-combined with the element
+    // offsets; the tile address is added afterwards)
+    const uint32_t sb = (uint32_t)swz(tbase) << 4;
+    const uint64_t gbase = tile_base | (uint64_t)(tbase & 15) | ((uint64_t)(tbase >> 4) << h);
+    double2 a[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const uint32_t addr = tile_a + (sb ^ (uint32_t)rd.eoff[e]);
+        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(a[e].x), "=d"(a[e].y) : "r"(addr));
+    }
+    if (rd.op_begin < rd.op_end) {
+        FusedOp nxt = ops[rd.op_begin];
+        const double *ncp = coef_of(nxt);
+        double nc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) nc[q] = ncp[q];
+        for (int o = rd.op_begin; o < rd.op_end; ++o) {
+            const FusedOp op = nxt;
+            const double *cp = ncp;
+            double cc[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) cc[q] = nc[q];
+            if (o + 1 < rd.op_end) {
+                nxt = ops[o + 1];
+                ncp = coef_of(nxt);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) nc[q] = ncp[q];
+            }
+            apply_fused_op<EXT>(a, op, cc, cp, gbase, rd.gpos);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const uint32_t addr = tile_a + (sb ^ (uint32_t)rd.eoff[e]);
+        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(a[e].x), "d"(a[e].y)
+                     : "memory");
+    }
+}
+
+// Bounded wait on an mbarrier phase.  Returns false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 24); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace lq

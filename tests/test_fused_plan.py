@@ -1,0 +1,52 @@
+"""CPU: the fused planner and encoder (via lq_plan_dump) against the oracle,
+through a numpy emulator of the kernel's addressing and register ops."""
+import numpy as np
+import pytest
+
+import oracle
+import fused_emulator as fe
+from helpers import random_state
+from logosq_b200 import abi, workloads
+from logosq_b200.gates import make_desc
+
+ONE_Q = [abi.H, abi.X, abi.Y, abi.Z, abi.S, abi.T, abi.RX, abi.RY, abi.RZ, abi.PHASE, abi.U3]
+TWO_Q = [abi.CNOT, abi.SWAP, abi.CZ, abi.CPHASE, abi.CRX, abi.CRY, abi.CRZ, abi.CPHASE_PARAM,
+         abi.RXX, abi.RYY, abi.RZZ]
+
+
+def random_circuit(n, count, seed):
+    rng = workloads.SplitMix64(seed)
+    recs = []
+    for _ in range(count):
+        kind = [*ONE_Q, *TWO_Q, abi.TOFFOLI][rng.randint(0, len(ONE_Q) + len(TWO_Q))]
+        k = 3 if kind == abi.TOFFOLI else (2 if kind in TWO_Q else 1)
+        qs = []
+        while len(qs) < k:
+            q = rng.randint(0, n - 1)
+            if q not in qs:
+                qs.append(q)
+        recs.append(make_desc(kind, qs, [rng.uniform(-3, 3) for _ in range(3)]))
+    return np.concatenate(recs)
+
+
+@pytest.mark.parametrize("n,seed", [(7, 1), (9, 2), (13, 3), (14, 14), (15, 5), (16, 6)])
+def test_emulated_random_circuits_match_oracle(n, seed):
+    g = random_circuit(n, 40 + 3 * n, seed)
+    v = random_state(n, seed)
+    assert np.abs(fe.run(n, g, v) - oracle.apply_circuit(v.copy(), g)).max() < 1e-12
+
+
+@pytest.mark.parametrize("n", [7, 12, 16])
+def test_emulated_qft_and_brickwork(n):
+    v = random_state(n, 1)
+    for g in (workloads.qft_gates(n), workloads.brickwork_u3(n, 6, seed=2)):
+        assert np.abs(fe.run(n, g, v) - oracle.apply_circuit(v.copy(), g)).max() < 1e-12
+
+
+def test_plan_uses_few_passes_for_brickwork():
+    import ctypes as C
+    from logosq_b200._lib import call
+    g = workloads.brickwork_u3(30, 20, seed=2)
+    p, r, s = C.c_int(), C.c_int(), C.c_int()
+    call("lq_plan_circuit", 30, abi.gate_ptr(g), len(g), C.byref(p), C.byref(r), C.byref(s))
+    assert s.value == 0 and p.value <= 20  # at most one HBM pass per layer
