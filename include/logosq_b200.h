@@ -326,9 +326,10 @@ int lq_batch_num_params(const lq_batch *b, int *out);
  * gets E(theta), grad[total params] the parameter-shift gradient. */
 int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *energy,
                        double *grad);
-/* Tuning chosen by the batch autotuner: states per CTA tile limit and the
- * fused-gate width used for shared-memory resident instances. */
-int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *threads_per_cta);
+/* Tuning of the batch: the largest qubit count kept entirely in shared memory,
+ * and the fusion width (tile bits) the autotuner chose on the first
+ * lq_batch_gradients call for larger instances (0 before that call). */
+int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits);
 
 #ifdef __cplusplus
 }

@@ -48,8 +48,13 @@ void resolve_locked() {
 
 bool prof_enabled() { return g_on; }
 
+static bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
 void prof_begin(cudaStream_t st, int cls) {
-    if (!g_on) return;
+    if (!g_on || capturing(st)) return;
     std::lock_guard<std::mutex> lk(g_mu);
     t_begin = take_event();
     t_cls = cls;
@@ -57,7 +62,7 @@ void prof_begin(cudaStream_t st, int cls) {
 }
 
 void prof_end(cudaStream_t st, int cls) {
-    if (!g_on || !t_begin || t_cls != cls) return;
+    if (!g_on || !t_begin || t_cls != cls || capturing(st)) return;
     std::lock_guard<std::mutex> lk(g_mu);
     cudaEvent_t e = take_event();
     cudaEventRecord(e, st);
