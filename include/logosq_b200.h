@@ -227,6 +227,25 @@ int lq_measure_shots(const lq_state *s, uint64_t n_shots, uint64_t seed, uint64_
 int lq_expectation_pauli(const lq_state *s, const lq_pauli_term *terms, int nterms,
                          int y_convention, double *out, double *per_term);
 
+/* Pauli-sum expectation that allocates no memory (no reference counterpart).
+ * For callers that cannot call cudaMalloc: code whose device memory is owned by
+ * a host framework's own allocator or strict memory budget, and code that must
+ * not insert the device-wide synchronisation an allocation or free can cause
+ * in the middle of its stream work.  Same result as lq_expectation_pauli, but
+ * the amplitudes are a caller-owned device pointer (2^num_qubits complex
+ * values of dtype LQ_C128 or LQ_C64), the work runs on the caller's CUDA
+ * stream (a cudaStream_t, NULL for the default stream) and all scratch lives
+ * in one fixed 64 KiB device array inside this library (every GPU that loads
+ * the library holds it until the process exits).  At most 1024 terms per call;
+ * more returns LQ_ERR_UNSUPPORTED.  The first call on each device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * Calls share the array: two calls whose work overlaps on the GPU race, so
+ * serialise them (one stream, or synchronise between them).  The call returns
+ * after the result is in *out. */
+int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dtype,
+                                const lq_pauli_term *terms, int nterms, int y_convention,
+                                void *stream, double *out);
+
 /* ---------------------------------------------------------------------------
  * Gates (src/gates/*.rs) -- each call is one in-place sweep on the state's
  * stream, the drop-in for Gate::apply (src/gates/mod.rs:26-35).

@@ -64,6 +64,8 @@ _PROTOS = {
     "lq_inner_product": (C.c_int, [_P, _P, _PD]),
     "lq_measure_shots": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     "lq_expectation_pauli": (C.c_int, [_P, _PT, C.c_int, C.c_int, _PD, _PD]),
+    "lq_expectation_pauli_static": (C.c_int, [_P, C.c_int, C.c_int, _PT, C.c_int, C.c_int, _P,
+                                              _PD]),
     "lq_apply_gate": (C.c_int, [_P, _PG, _PD, C.c_int]),
     "lq_apply_matrix1": (C.c_int, [_P, C.c_int, _PD]),
     "lq_apply_controlled1": (C.c_int, [_P, C.c_int, C.c_int, _PD]),

@@ -428,11 +428,138 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
     return LQ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Pauli-sum expectation that allocates nothing (lq_expectation_pauli_static).
+//
+// Its scratch -- the per-block partial sums, the per-group results and the
+// packed term coefficients -- lives in one file-scope device array of fixed
+// size instead of memory obtained from cudaMalloc.  Host code cannot hand the
+// array's name to a kernel (on the host that name is only a stand-in, not a
+// device address), so the device address is fetched once per device with
+// cudaGetSymbolAddress and cached.
+// ---------------------------------------------------------------------------
+constexpr int kStaticMaxTerms = 1024;
+constexpr size_t kStaticPartialBytes = sizeof(double) * kRedBlocks;
+constexpr size_t kStaticResultBytes = sizeof(double) * kStaticMaxTerms;
+constexpr size_t kStaticCoefBytes = sizeof(TermCoef) * kStaticMaxTerms;
+constexpr size_t kStaticScratchBytes = 64 * 1024;
+static_assert(kStaticPartialBytes + kStaticResultBytes + kStaticCoefBytes <= kStaticScratchBytes,
+              "static scratch too small");
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+static int static_scratch_address(unsigned char **out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static unsigned char *addr[kMaxDevices] = {};
+    int dev = 0;
+    LQ_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(LQ_ERR_UNSUPPORTED, "device %d", dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(LQ_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s",
+                             cudaGetErrorString(e));
+        addr[dev] = (unsigned char *)p;
+    }
+    *out = addr[dev];
+    return LQ_OK;
+}
+
 }  // namespace lq
 
 using namespace lq;
 
 extern "C" {
+
+int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dtype,
+                                const lq_pauli_term *terms, int nterms, int y_convention,
+                                void *stream, double *out) {
+    if (!d_amplitudes || !out || (nterms > 0 && !terms) || nterms < 0)
+        return set_error(LQ_ERR_INVALID_ARG, "null pointer or negative term count");
+    if (num_qubits < 1 || num_qubits > 36)
+        return set_error(LQ_ERR_STATE_DIMENSION, "num_qubits %d outside 1..36", num_qubits);
+    if (dtype != LQ_C128 && dtype != LQ_C64)
+        return set_error(LQ_ERR_INVALID_ARG, "unknown dtype %d", dtype);
+    if (y_convention != LQ_Y_REFERENCE && y_convention != LQ_Y_TEXTBOOK)
+        return set_error(LQ_ERR_INVALID_ARG, "unknown Y convention %d", y_convention);
+    if (nterms > kStaticMaxTerms)
+        return set_error(LQ_ERR_UNSUPPORTED,
+                         "%d Pauli terms exceed the fixed scratch of this entry point "
+                         "(at most %d terms; use lq_expectation_pauli)",
+                         nterms, kStaticMaxTerms);
+    if (nterms == 0) {
+        *out = 0.0;
+        return LQ_OK;
+    }
+    const int n = num_qubits;
+    const uint64_t lim = n == 64 ? ~0ull : ((1ull << n) - 1);
+    for (int t = 0; t < nterms; ++t) {
+        if ((terms[t].xmask & ~lim) || (terms[t].zmask & ~lim))
+            return set_error(LQ_ERR_QUBIT_INDEX, "Pauli term %d acts on a qubit >= %d", t, n);
+        if (terms[t].ny != __builtin_popcountll(terms[t].xmask & terms[t].zmask))
+            return set_error(LQ_ERR_INVALID_ARG, "Pauli term %d: ny does not match its masks", t);
+    }
+    unsigned char *scratch = nullptr;
+    LQ_TRY(static_scratch_address(&scratch));
+    double *d_partials = (double *)scratch;
+    double *d_results = (double *)(scratch + kStaticPartialBytes);
+    TermCoef *d_coef = (TermCoef *)(scratch + kStaticPartialBytes + kStaticResultBytes);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    // Group the terms by X mask with fixed-size host arrays (no heap).
+    int order[kStaticMaxTerms], gbegin[kStaticMaxTerms + 1];
+    uint64_t gx[kStaticMaxTerms];
+    bool used[kStaticMaxTerms] = {};
+    int ng = 0, k = 0;
+    for (int t = 0; t < nterms; ++t) {
+        if (used[t]) continue;
+        gx[ng] = terms[t].xmask;
+        gbegin[ng] = k;
+        for (int u = t; u < nterms; ++u)
+            if (!used[u] && terms[u].xmask == gx[ng]) {
+                used[u] = true;
+                order[k++] = u;
+            }
+        ++ng;
+    }
+    gbegin[ng] = k;
+    TermCoef packed[kStaticMaxTerms];  // host stack: 24 KiB
+    for (int i = 0; i < nterms; ++i) {
+        const lq_pauli_term &pt = terms[order[i]];
+        int q = pt.ny & 3;
+        if (y_convention == LQ_Y_TEXTBOOK) q = (4 - q) & 3;
+        const double a = q == 0 ? 1.0 : q == 2 ? -1.0 : 0.0;
+        const double b = q == 1 ? -1.0 : q == 3 ? 1.0 : 0.0;
+        packed[i] = TermCoef{pt.zmask, pt.coefficient * a, pt.coefficient * b};
+    }
+    LQ_CUDA_TRY(cudaMemcpyAsync(d_coef, packed, sizeof(TermCoef) * nterms,
+                                cudaMemcpyHostToDevice, st));
+    const uint64_t N = 1ull << n;
+    const int th = 256;
+    const int g = red_grid(std::max<uint64_t>(N / 2, 1), th);
+    for (int gi = 0; gi < ng; ++gi) {
+        const int nt = gbegin[gi + 1] - gbegin[gi];
+        const size_t shm = nt * sizeof(TermCoef);
+        if (dtype == LQ_C128)
+            k_pauli_group<<<g, th, shm, st>>>((const double2 *)d_amplitudes, n, gx[gi],
+                                              d_coef + gbegin[gi], nt, d_partials);
+        else
+            k_pauli_group<<<g, th, shm, st>>>((const float2 *)d_amplitudes, n, gx[gi],
+                                              d_coef + gbegin[gi], nt, d_partials);
+        k_final_sum<1><<<1, 256, 0, st>>>(d_partials, g, d_results + gi);
+    }
+    LQ_CUDA_TRY(cudaGetLastError());
+    double res[kStaticMaxTerms];  // host stack: 8 KiB
+    LQ_CUDA_TRY(cudaMemcpyAsync(res, d_results, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+    LQ_CUDA_TRY(cudaStreamSynchronize(st));
+    double sum = 0.0;
+    for (int gi = 0; gi < ng; ++gi) sum += res[gi];
+    *out = sum;
+    return LQ_OK;
+}
 
 const char *lq_last_error(void) { return g_last_error.c_str(); }
 

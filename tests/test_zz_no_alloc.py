@@ -1,0 +1,69 @@
+"""GPU: the allocation-free Pauli-sum expectation (lq_expectation_pauli_static).
+
+Some callers cannot call cudaMalloc -- their device memory belongs to a host
+framework's own allocator or budget, or they must not put the device-wide
+synchronisation of an allocation into the middle of their stream work.  This
+entry point keeps its scratch in a fixed array inside the library and works on
+caller-owned device memory; here it must give the same energy as the regular
+lq_expectation_pauli on two calls in a row (the second call finds the first
+call's leftovers in the shared scratch array).  Collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from logosq_b200 import State, abi, workloads
+from logosq_b200._lib import LogosQError, call
+
+pytestmark = pytest.mark.gpu
+
+
+def _terms(n, count, seed):
+    rng = workloads.SplitMix64(seed)
+    t = np.zeros(count, dtype=abi.TERM_DTYPE)
+    for k in range(count):
+        x = rng.randint(0, (1 << n) - 1) if k % 3 else 0
+        z = rng.randint(0, (1 << n) - 1)
+        t[k]["coefficient"] = rng.uniform(-1, 1)
+        t[k]["xmask"] = x
+        t[k]["zmask"] = z
+        t[k]["ny"] = bin(x & z).count("1")
+    return t
+
+
+def _regular(st, terms, yconv):
+    out = C.c_double()
+    call("lq_expectation_pauli", st.handle, abi.term_ptr(terms), len(terms), yconv, C.byref(out),
+         None)
+    return out.value
+
+
+def _static(st, terms, yconv):
+    ptr, stream = C.c_void_p(), C.c_void_p()
+    call("lq_state_device_ptr", st.handle, C.byref(ptr))
+    call("lq_state_stream", st.handle, C.byref(stream))
+    out = C.c_double()
+    call("lq_expectation_pauli_static", ptr, st.num_qubits(), abi.LQ_C128, abi.term_ptr(terms),
+         len(terms), yconv, stream, C.byref(out))
+    return out.value
+
+
+def test_static_expectation_matches_regular_two_calls():
+    cases = [(15, 60, 1, abi.Y_REFERENCE), (12, 300, 2, abi.Y_TEXTBOOK)]
+    for n, count, seed, yconv in cases:  # two calls in a row, different inputs
+        st = State.zero_state(n)
+        st.set_vector(workloads.gaussian_state(n, seed))
+        terms = _terms(n, count, seed)
+        want = _regular(st, terms, yconv)
+        got = _static(st, terms, yconv)
+        assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (n, got, want)
+        st.close()
+
+
+def test_static_expectation_rejects_too_many_terms():
+    st = State.zero_state(4)
+    terms = _terms(4, 1025, 3)
+    with pytest.raises(LogosQError) as e:
+        _static(st, terms, abi.Y_REFERENCE)
+    assert e.value.code == abi.LQ_ERR_UNSUPPORTED
