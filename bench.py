@@ -207,6 +207,109 @@ def run_vqe_batch(args):
     return 0
 
 
+class _DevArray:
+    """A raw device buffer exposed through __cuda_array_interface__ (used only to
+    compare two engine states on the device)."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3}
+
+
+def run_precision(args):
+    """Precision form: complex64 state, 20-layer U3+CNOT brickwork (seed 3) fused
+    into 5-qubit blocks on tcgen05 (3xTF32).  Times the 32-qubit run and checks
+    the FP64 norm and Z...Z energy; at 30 qubits compares amplitudes and energy
+    with the complex128 engine on the same circuit."""
+    import torch
+    from logosq_b200 import State, abi, workloads
+    from logosq_b200._lib import call
+
+    def zz_energy(st, n):
+        t = np.zeros(1, dtype=abi.TERM_DTYPE)
+        t["coefficient"] = 1.0
+        t["zmask"] = np.uint64((1 << n) - 1)
+        e = C.c_double()
+        call("lq_expectation_pauli", st.handle, abi.term_ptr(t), 1, abi.Y_REFERENCE, C.byref(e),
+             None)
+        return e.value
+
+    def run_tc(n, layers, steps, warmup):
+        g = workloads.brickwork_u3(n, layers, seed=3)
+        st = State.zero_state(n, dtype=abi.LQ_C64)
+        nb, npass = C.c_int(), C.c_int()
+        sp = C.c_void_p()
+        call("lq_state_stream", st.handle, C.byref(sp))
+        stream = torch.cuda.ExternalStream(sp.value)
+        for _ in range(warmup):
+            call("lq_state_set_basis", st.handle, C.c_uint64(0))
+            call("lq_apply_circuit_tc", st.handle, n, abi.gate_ptr(g), len(g), None, 0,
+                 C.byref(nb), C.byref(npass))
+        st.synchronize()
+        call("lq_profile_enable", 1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call("lq_state_set_basis", st.handle, C.c_uint64(0))
+            call("lq_apply_circuit_tc", st.handle, n, abi.gate_ptr(g), len(g), None, 0,
+                 C.byref(nb), C.byref(npass))
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / max(steps, 1)
+        tc_ms, tc_n = C.c_double(), C.c_longlong()
+        call("lq_profile_read", 4, C.byref(tc_ms), C.byref(tc_n))
+        call("lq_profile_enable", 0)
+        return st, g, ms, nb.value, npass.value, tc_ms.value / max(tc_n.value, 1)
+
+    n = args.qubits if args.qubits != 30 else 32
+    st32, g32, ms, nblocks, npasses, launch_ms = run_tc(n, 20, args.steps, args.warmup)
+    norm32 = st32.norm_sqr()
+    e32 = zz_energy(st32, n)
+    S = 8 << n
+    # 3xTF32: 3 real 128x64x64 GEMMs per 128 rows of 32 amplitudes
+    flops_per_block = 3 * 2 * 64 * 64 * (1 << n) // 32 * 2
+    st32.close()
+    # 30-qubit comparison against the complex128 engine
+    m = 30
+    st64, g30, _, _, _, _ = run_tc(m, 20, 1, 0)
+    ref = State.zero_state(m)
+    call("lq_apply_circuit", ref.handle, m, abi.gate_ptr(g30), len(g30), None, 0, abi.EXEC_FUSED)
+    p64, p128 = C.c_void_p(), C.c_void_p()
+    call("lq_state_device_ptr", st64.handle, C.byref(p64))
+    call("lq_state_device_ptr", ref.handle, C.byref(p128))
+    st64.synchronize()
+    ref.synchronize()
+    a = torch.as_tensor(_DevArray(p64.value, 2 << m, "<f4"), device="cuda")
+    b = torch.as_tensor(_DevArray(p128.value, 2 << m, "<f8"), device="cuda")
+    maxabs = 0.0
+    chunk = 1 << 28
+    for o in range(0, 2 << m, chunk):
+        d = (a[o:o + chunk].double() - b[o:o + chunk]).abs().max().item()
+        maxabs = max(maxabs, d)
+    amp_scale = float(b.abs().max().item())
+    e30_tc, e30_ref = zz_energy(st64, m), zz_energy(ref, m)
+    norm30 = st64.norm_sqr()
+    line = {"metric": f"precision form {n}q complex64 gate-layer GB/s (tcgen05 3xTF32 blocks)",
+            "value": workloads.brickwork_bytes(n, 20, amp_bytes=8) / (ms / 1e3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "tf32x3 -> f32 (complex64)",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"U3+CNOT brickwork, {n} qubits complex64, 20 layers, seed 3",
+                       "blocks_per_step": nblocks, "passes_per_step": npasses},
+            "roofline": {"kernel": "k_tc_pass", "bound": "hbm", "avg_launch_ms": launch_ms,
+                         "achieved": 2 * S / (launch_ms / 1e3) / 1e9, "unit": "GB/s",
+                         "peak": hbm_peak()[0],
+                         "frac": 2 * S / (launch_ms / 1e3) / 1e9 / hbm_peak()[0],
+                         "tensor_tflops_issued": flops_per_block * nblocks / (ms / 1e3) / 1e12},
+            "fp64_norm": norm32, "fp64_zstring_energy": e32,
+            "check_30q": {"max_abs_amplitude_error": maxabs, "max_abs_amplitude": amp_scale,
+                          "zstring_energy_tc": e30_tc, "zstring_energy_c128": e30_ref,
+                          "energy_abs_error": abs(e30_tc - e30_ref), "fp64_norm_tc": norm30}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,11 +330,14 @@ def main():
     ap.add_argument("--per-gate-steps", type=int, default=1)
     ap.add_argument("--fusion-width", type=int, default=0,
                     help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
-    ap.add_argument("--workload", default="brickwork", choices=["brickwork", "vqe-batch"])
+    ap.add_argument("--workload", default="brickwork",
+                    choices=["brickwork", "vqe-batch", "precision"])
     ap.add_argument("--instances", type=int, default=256)
     args = ap.parse_args()
     if args.workload == "vqe-batch":
         return run_vqe_batch(args)
+    if args.workload == "precision":
+        return run_precision(args)
     n, layers = args.qubits, args.layers
     ws, rank, local = dist_info()
     metric = f"{n}q gate-layer GB/s"

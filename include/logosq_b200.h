@@ -297,6 +297,14 @@ int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, i
  * records and the FP64 coefficients.  *used receives the size needed. */
 int lq_plan_dump(int num_qubits, const lq_gate *ops, int nops, const double *theta, int ntheta,
                  void *buf, size_t cap, size_t *used);
+/* Precision form: Circuit::execute on a complex64 state (LQ_C64, n >= 12) with
+ * the gates fused into 5-qubit blocks, each applied as a complex 32 x 32 GEMM
+ * on the tcgen05 tensor cores (TF32 inputs, 3xTF32 split products, FP32
+ * accumulation).  Gates must act on at most 2 qubits.  *blocks / *passes
+ * (optional) receive the number of 5-qubit blocks and of full-state passes.
+ * FP64 is kept for lq_norm_sqr / lq_expectation_pauli on the result. */
+int lq_apply_circuit_tc(lq_state *s, int circuit_qubits, const lq_gate *ops, int nops,
+                        const double *theta, int ntheta, int *blocks, int *passes);
 /* Statistics of the last lq_apply_circuit on this handle: number of kernel
  * launches and number of fused passes (0 in per-gate mode). */
 int lq_last_circuit_stats(const lq_state *s, int *launches, int *passes);

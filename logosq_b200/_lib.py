@@ -75,6 +75,7 @@ _PROTOS = {
     "lq_apply_block": (C.c_int, [_P, C.c_int, _PI, _PD]),
     "lq_apply_circuit": (C.c_int, [_P, C.c_int, _PG, C.c_int, _PD, C.c_int, C.c_int]),
     "lq_last_circuit_stats": (C.c_int, [_P, _PI, _PI]),
+    "lq_apply_circuit_tc": (C.c_int, [_P, C.c_int, _PG, C.c_int, _PD, C.c_int, _PI, _PI]),
     "lq_plan_circuit": (C.c_int, [C.c_int, _PG, C.c_int, _PI, _PI, _PI]),
     "lq_set_fusion_width": (C.c_int, [C.c_int]),
     "lq_get_fusion_width": (C.c_int, [_PI]),

@@ -24,6 +24,7 @@ SOURCES = [
     "variational.cu",
     "profile.cu",
     "batch.cu",
+    "tc.cu",
 ]
 
 NVCC_FLAGS = [

@@ -1,0 +1,608 @@
+// Precision form: complex64 state, gates fused into 5-qubit blocks applied as
+// complex 32x32 GEMMs on the 5th-generation tensor cores (tcgen05, TF32 inputs,
+// FP32 accumulation in tensor memory) with the 3xTF32 split
+//     X W ~= Xh Wh + Xh Wl + Xl Wh,   Xh = tf32(X), Xl = tf32(X - Xh).
+//
+// A pass owns a window of T = 12 index bits ([0,4) U [h, h+8), as the FP64
+// fused passes).  Each CTA stages one 2^12-amplitude complex64 tile (32 KiB) by
+// TMA (128-byte swizzle) and applies the pass's blocks in order.  For a block
+// on tile bits k0..k4 the tile is a 128 x 32 complex matrix X (rows: the other
+// seven tile bits; columns: the block index).  Viewed as reals interleaved
+// (re, im) it is X' (128 x 64) and the block is Y' = X' W' with the real
+// 64 x 64 matrix W' = [[Re U^T, Im U^T], [-Im U^T, Re U^T]] interleaved the
+// same way.  The 128 threads gather X' into two K-major 128-byte-swizzled
+// operand buffers (hi and lo TF32 parts), one elected thread issues 3 x 8
+// tcgen05.mma (K = 8 each) into a 128-lane x 64-column FP32 accumulator in
+// TMEM, commits to an mbarrier, and each warp reads its 32 lanes back with
+// tcgen05.ld and scatters the rows into the tile.  The tile is written back
+// by one TMA store.  W' hi/lo are prepared on the host (FP64 -> TF32 splits)
+// already in the swizzled byte order of the B operand.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <complex>
+#include <cstring>
+#include <mutex>
+
+#include "fused_plan.h"
+
+namespace lq {
+
+constexpr int kTcT = 12;                // tile bits
+constexpr int kTcRows = 1 << (kTcT - 5);  // 128 GEMM rows per tile
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTileBytes = 8u << kTcT;          // 32 KiB complex64 tile
+constexpr uint32_t kABytes = kTcRows * 64 * 4;       // 32 KiB per A part (hi / lo)
+constexpr uint32_t kBBytes = 64 * 64 * 4;            // 16 KiB per B part (hi / lo)
+constexpr uint32_t kTcSmem = kTileBytes + 2 * kABytes + 2 * kBBytes + 1024 + 64;
+
+struct TcBlock {
+    int32_t k[5];     // tile-local bit of block bit j (block index bit j)
+    int32_t pad[3];
+    uint32_t row_bits[7];  // tile-local positions of the 7 row bits
+    uint32_t pad2;
+    uint64_t b_offset;  // offset (bytes) of this block's 32 KiB B image (hi then lo)
+};
+
+struct TcPass {
+    int32_t h;
+    int32_t block_begin, nblocks;
+    int32_t pad;
+};
+
+__device__ __forceinline__ uint32_t tc_smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Byte offset of complex64 tile element l in the TMA 128-byte-swizzled tile:
+// 128-byte rows hold 16 amplitudes (bits 0-3); 16-byte chunks hold 2.
+__device__ __forceinline__ uint32_t tile_off(uint32_t l) {
+    const uint32_t row = l >> 4, chunk = (l & 15) >> 1;
+    return row * 128 + ((chunk ^ (row & 7)) << 4) + ((l & 1) << 3);
+}
+
+// Byte offset of K-major operand element (row m, float k), rows of 128 B per
+// K-atom of 32 floats, 128-byte swizzle, atoms of `rows` rows.
+__device__ __forceinline__ uint32_t kmajor_off(uint32_t m, uint32_t k, uint32_t rows) {
+    const uint32_t atom = k >> 5, kb = (k & 31) * 4;
+    return atom * rows * 128 + m * 128 + (((kb >> 4) ^ (m & 7)) << 4) + (kb & 15);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ uint64_t make_sdesc(uint32_t addr, uint32_t sbo_bytes) {
+    // tcgen05 shared-memory descriptor: start address >> 4 [0,14), leading
+    // byte offset (unused for swizzled K-major, 1) [16,30), stride byte offset
+    // >> 4 [32,46), version 1 [46,48), layout SWIZZLE_128B (2) [61,64).
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 24); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, N = 64, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_tc_pass(const __grid_constant__ CUtensorMap tmap, int32_t h, int32_t hm,
+              const TcBlock *__restrict__ blocks, int nblocks,
+              const unsigned char *__restrict__ bimg, unsigned *__restrict__ flag) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *tile = base;
+    unsigned char *a_hi = tile + kTileBytes;
+    unsigned char *a_lo = a_hi + kABytes;
+    unsigned char *b_hi = a_lo + kABytes;
+    unsigned char *b_lo = b_hi + kBBytes;
+    uint64_t *bars = (uint64_t *)(b_lo + kBBytes);  // [0] TMA load, [1] MMA done
+    uint32_t *tmem_slot = (uint32_t *)(bars + 2);
+    const uint32_t tile_a = tc_smem_u32(tile);
+    const uint32_t bar_load = tc_smem_u32(&bars[0]);
+    const uint32_t bar_mma = tc_smem_u32(&bars[1]);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int32_t bid = blockIdx.x;
+    const int32_t c1 = bid & ((1 << (h - 4)) - 1);
+    const int32_t c3 = bid >> (h - 4);
+    const int32_t zero = 0;
+    bool ok = true;
+
+    if (warp == 0) {
+        // 64 TMEM columns for the 128 x 64 FP32 accumulator
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         tc_smem_u32(tmem_slot)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_load), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_mma), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_load),
+                     "r"(kTileBytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(tile_a),
+            "l"((uint64_t)&tmap), "r"(zero), "r"(c1), "r"(zero), "r"(c3), "r"(bar_load)
+            : "memory");
+    }
+    if (!tc_wait(bar_load, 0)) ok = false;
+
+    uint32_t mma_phase = 0;
+    for (int bi = 0; bi < nblocks && ok; ++bi) {
+        const TcBlock blk = blocks[bi];
+        // B operand (hi, lo): prepared swizzled image, plain 16-byte copies
+        {
+            const uint4 *src = (const uint4 *)(bimg + blk.b_offset);
+            uint4 *dst = (uint4 *)b_hi;  // b_hi and b_lo are contiguous
+            for (int i = tid; i < (int)(2 * kBBytes / 16); i += kTcThreads) dst[i] = src[i];
+        }
+        // A operand: row m = tid, the 32 complex entries of the block
+        {
+            const uint32_t m = tid;
+            uint32_t lbase = 0;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) lbase |= ((m >> j) & 1u) << blk.row_bits[j];
+#pragma unroll 4
+            for (uint32_t c = 0; c < 32; ++c) {
+                uint32_t l = lbase;
+#pragma unroll
+                for (int j = 0; j < 5; ++j) l |= ((c >> j) & 1u) << blk.k[j];
+                const float2 v = *(const float2 *)(tile + tile_off(l));
+                const float rh = to_tf32(v.x), ih = to_tf32(v.y);
+                const float rl = to_tf32(v.x - rh), il = to_tf32(v.y - ih);
+                const uint32_t o0 = kmajor_off(m, 2 * c, kTcRows);
+                const uint32_t o1 = kmajor_off(m, 2 * c + 1, kTcRows);
+                *(float *)(a_hi + o0) = rh;
+                *(float *)(a_hi + o1) = ih;
+                *(float *)(a_lo + o0) = rl;
+                *(float *)(a_lo + o1) = il;
+            }
+        }
+        // generic-proxy smem writes -> visible to the tensor-core (async) proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            const uint32_t ah = tc_smem_u32(a_hi), al = tc_smem_u32(a_lo);
+            const uint32_t bh = tc_smem_u32(b_hi), bl = tc_smem_u32(b_lo);
+            const uint32_t pa[3] = {ah, ah, al}, pb[3] = {bh, bl, bh};
+#pragma unroll
+            for (int prod = 0; prod < 3; ++prod) {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    // K step kk: 8 TF32 = 32 bytes; atom = kk / 4
+                    const uint32_t aoff = (kk >> 2) * (kTcRows * 128) + (kk & 3) * 32;
+                    const uint32_t boff = (kk >> 2) * (64 * 128) + (kk & 3) * 32;
+                    const uint64_t da = make_sdesc(pa[prod] + aoff, 1024);
+                    const uint64_t db = make_sdesc(pb[prod] + boff, 1024);
+                    const uint32_t acc = (prod | kk) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+                            tmem),
+                        "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+                        : "memory");
+                }
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    bar_mma)
+                : "memory");
+        }
+        if (!tc_wait(bar_mma, mma_phase)) {
+            // give the tensor-core work in flight a second bounded wait before
+            // the accumulator columns are released below
+            tc_wait(bar_mma, mma_phase);
+            ok = false;
+            break;
+        }
+        mma_phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // D rows back: warp w owns TMEM lanes 32w..32w+31; thread = row tid
+        {
+            float d[64];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + q * 16;
+                uint32_t r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, "
+                    "%8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                      "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                      "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr));
+#pragma unroll
+                for (int i = 0; i < 16; ++i) d[q * 16 + i] = __uint_as_float(r[i]);
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const uint32_t m = tid;
+            uint32_t lbase = 0;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) lbase |= ((m >> j) & 1u) << blk.row_bits[j];
+#pragma unroll
+            for (uint32_t c = 0; c < 32; ++c) {
+                uint32_t l = lbase;
+#pragma unroll
+                for (int j = 0; j < 5; ++j) l |= ((c >> j) & 1u) << blk.k[j];
+                *(float2 *)(tile + tile_off(l)) = make_float2(d[2 * c], d[2 * c + 1]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        (void)lane;
+    }
+    if (ok) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile(
+                "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group"
+                " [%0, {%1, %2, %3, %4}], [%5];" ::"l"((uint64_t)&tmap),
+                "r"(zero), "r"(c1), "r"(zero), "r"(c3), "r"(tile_a)
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        }
+    } else if (tid == 0) {
+        atomicOr(flag, kFlagTimeout);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64)
+                     : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 tc_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// complex64 tile map for the window [0,4) U [h, h+8):
+//   dim0: 32 floats (16 amplitudes, bits 0-3), box 32 (128 B)
+//   dim1: 2^(h-4) (bits 4..h-1), box 1
+//   dim2: 2^8 (bits h..h+7), box 256
+//   dim3: 2^(n-h-8) (bits h+8..), box 1
+static int tc_tile_map(CUtensorMap *map, void *d, int n, int h) {
+    auto enc = tc_encode();
+    if (!enc) return set_error(LQ_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    cuuint64_t dims[4] = {32, 1ull << (h - 4), 256, 1ull << (n - h - 8)};
+    cuuint64_t strides[3] = {128, 8ull << h, 8ull << (h + 8)};
+    cuuint32_t box[4] = {32, 1, 256, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return set_error(LQ_ERR_CUDA, "cuTensorMapEncodeTiled (complex64) failed (%d)", (int)r);
+    return LQ_OK;
+}
+
+using cd = std::complex<double>;
+
+// Apply canonical op g (global index bits) to a 32-dim vector whose block bit j
+// corresponds to global bit gbit[j].
+static void small_apply(const GateOp &g, const int gbit[5], cd *v) {
+    auto loc = [&](int b) {
+        for (int j = 0; j < 5; ++j)
+            if (gbit[j] == b) return j;
+        return -1;
+    };
+    auto c = [&](int k) { return cd(g.m[2 * k], g.m[2 * k + 1]); };
+    switch (g.type) {
+    case OP_M1:
+    case OP_PERM1: {
+        const int t = loc(g.t);
+        int cm = 0;
+        for (int k = 0; k < g.nctrl; ++k) cm |= 1 << loc(g.ctrl[k]);
+        for (int e = 0; e < 32; ++e) {
+            if ((e >> t) & 1) continue;
+            if ((e & cm) != cm) continue;
+            const int f = e | (1 << t);
+            const cd a0 = v[e], a1 = v[f];
+            if (g.type == OP_PERM1) {
+                v[e] = a1;
+                v[f] = a0;
+            } else {
+                v[e] = c(0) * a0 + c(1) * a1;
+                v[f] = c(2) * a0 + c(3) * a1;
+            }
+        }
+        break;
+    }
+    case OP_DIAG: {
+        int fm = 0;
+        for (int k = 0; k < g.nfix; ++k) fm |= 1 << loc(g.fix[k]);
+        for (int e = 0; e < 32; ++e) {
+            if ((e & fm) != fm) continue;
+            int pat = 0;
+            for (int k = 0; k < g.npat; ++k) pat |= ((e >> loc(g.pat[k])) & 1) << k;
+            v[e] *= c(pat);
+        }
+        break;
+    }
+    case OP_SWAP: {
+        const int a = loc(g.b0), b = loc(g.b1);
+        for (int e = 0; e < 32; ++e)
+            if (((e >> a) & 1) && !((e >> b) & 1)) std::swap(v[e], v[e ^ (1 << a) ^ (1 << b)]);
+        break;
+    }
+    case OP_M2: {
+        const int a = loc(g.b0), b = loc(g.b1);
+        for (int e = 0; e < 32; ++e) {
+            if (((e >> a) & 1) || ((e >> b) & 1)) continue;
+            const int idx[4] = {e, e | (1 << b), e | (1 << a), e | (1 << a) | (1 << b)};
+            cd in[4], out[4];
+            for (int r = 0; r < 4; ++r) in[r] = v[idx[r]];
+            for (int r = 0; r < 4; ++r) {
+                out[r] = 0;
+                for (int q = 0; q < 4; ++q) out[r] += cd(g.m[(r * 4 + q) * 2], g.m[(r * 4 + q) * 2 + 1]) * in[q];
+            }
+            for (int r = 0; r < 4; ++r) v[idx[r]] = out[r];
+        }
+        break;
+    }
+    }
+}
+
+static inline float host_tf32(double x) {
+    // round-to-nearest (ties away) to a 10-bit mantissa, as cvt.rna.tf32.f32
+    float f = (float)x;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) {
+        u += 0x1000u;
+        u &= 0xffffe000u;
+    }
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+// Swizzled byte image of B (N x K K-major, two K atoms of 64 rows x 128 B).
+static void write_b_image(const double W[64][64], unsigned char *hi, unsigned char *lo) {
+    for (int n = 0; n < 64; ++n)
+        for (int k = 0; k < 64; ++k) {
+            const int atom = k >> 5, kb = (k & 31) * 4;
+            const size_t off = (size_t)atom * 64 * 128 + n * 128 + (((kb >> 4) ^ (n & 7)) << 4) +
+                               (kb & 15);
+            const double w = W[k][n];
+            const float h = host_tf32(w);
+            const float l = host_tf32(w - (double)h);
+            memcpy(hi + off, &h, 4);
+            memcpy(lo + off, &l, 4);
+        }
+}
+
+struct TcPlan {
+    std::vector<PlanStep> steps;  // fused steps reuse the window; blocks below
+    std::vector<std::vector<std::vector<int>>> pass_blocks;  // per fused step: blocks of gates
+    std::vector<std::vector<std::vector<int>>> block_bits;   // per step/block: 5 global bits
+};
+
+// Split each window pass into 5-bit blocks: greedy in order, a gate joins the
+// open block when all its bits fit in <= 5 bits and no earlier skipped gate
+// shares a bit.
+static void tc_blocks(const std::vector<GateOp> &gops, const std::vector<int> &gates, int h,
+                      int T, std::vector<std::vector<int>> &blocks,
+                      std::vector<std::vector<int>> &bits) {
+    const int P = (int)gates.size();
+    std::vector<char> sched(P, 0);
+    int left = P;
+    while (left > 0) {
+        uint64_t B = 0, blk = 0;
+        std::vector<int> cur;
+        for (int k = 0; k < P; ++k) {
+            if (sched[k]) continue;
+            const uint64_t gb = op_bits(gops[gates[k]]);
+            if ((gb & blk) == 0 && __builtin_popcountll(B | gb) <= 5) {
+                B |= gb;
+                cur.push_back(gates[k]);
+                sched[k] = 1;
+                --left;
+            } else {
+                blk |= gb;
+            }
+        }
+        std::vector<int> bv;
+        for (int b = 0; b < 64; ++b)
+            if (B >> b & 1) bv.push_back(b);
+        // pad to five bits of the window
+        const uint64_t W = window_mask(h, T - 4);
+        for (int b = 0; b < 64 && bv.size() < 5; ++b)
+            if ((W >> b & 1) && !(B >> b & 1)) bv.push_back(b);
+        std::sort(bv.begin(), bv.end());
+        blocks.push_back(cur);
+        bits.push_back(bv);
+    }
+}
+
+int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const double *theta,
+                          int ntheta, int *nblocks_out, int *npasses_out) {
+    const int n = s->n;
+    if (s->dtype != LQ_C64)
+        return set_error(LQ_ERR_UNSUPPORTED, "the tensor-core path runs on complex64 states");
+    if (n < kTcT) return set_error(LQ_ERR_UNSUPPORTED, "the tensor-core path needs >= 12 qubits");
+    std::vector<GateOp> gops(nops);
+    for (int i = 0; i < nops; ++i) {
+        LQ_TRY(validate_gate(&ops[i], n, ntheta));
+        LQ_TRY(make_gate_op(&ops[i], theta, n, &gops[i]));
+        if (gops[i].renorm)
+            return set_error(LQ_ERR_UNSUPPORTED, "renormalising gates are not fused on tensor cores");
+    }
+    // Windows: the FP64 planner with every gate required fully inside the window
+    // (dense blocks cannot read controls outside it).
+    std::vector<GateOp> planner_ops = gops;
+    for (auto &g : planner_ops) {
+        // make every bit a mixed bit for window selection: widen to a 4x4-like op
+        if (g.type == OP_DIAG || g.nctrl > 0 || g.type == OP_PERM1) {
+            GateOp w = g;
+            w.type = OP_M2;
+            const uint64_t b = op_bits(g);
+            int bits[3], nb = 0;
+            for (int k = 0; k < 64 && nb < 3; ++k)
+                if (b >> k & 1) bits[nb++] = k;
+            if (nb == 1) {
+                w.type = OP_M1;
+                w.t = bits[0];
+                w.nctrl = 0;
+            } else if (nb == 2) {
+                w.b0 = bits[0];
+                w.b1 = bits[1];
+            } else {
+                return set_error(LQ_ERR_UNSUPPORTED, "3-qubit gates are not fused on tensor cores");
+            }
+            w.nfix = w.npat = 0;
+            g = w;
+        }
+    }
+    std::vector<PlanStep> steps = plan_circuit(planner_ops, n, kTcT);
+    std::vector<TcBlock> blocks;
+    std::vector<TcPass> passes;
+    std::vector<unsigned char> bimg;
+    std::vector<int> step_pass(steps.size(), -1);
+    for (size_t si = 0; si < steps.size(); ++si) {
+        const PlanStep &st = steps[si];
+        if (!st.fused) continue;
+        std::vector<std::vector<int>> bl, bb;
+        tc_blocks(gops, st.pass.gates, st.pass.h, kTcT, bl, bb);
+        TcPass tp{st.pass.h, (int)blocks.size(), (int)bl.size(), 0};
+        for (size_t b = 0; b < bl.size(); ++b) {
+            int gbit[5];
+            for (int j = 0; j < 5; ++j) gbit[j] = bb[b][j];
+            // block unitary U (32 x 32): column e = product of gates on basis e
+            cd U[32][32];
+            for (int e = 0; e < 32; ++e) {
+                cd v[32] = {};
+                v[e] = 1.0;
+                for (int gi : bl[b]) small_apply(gops[gi], gbit, v);
+                for (int r = 0; r < 32; ++r) U[r][e] = v[r];
+            }
+            double W[64][64];
+            for (int r = 0; r < 32; ++r)
+                for (int c = 0; c < 32; ++c) {
+                    W[2 * c][2 * r] = U[r][c].real();
+                    W[2 * c + 1][2 * r] = -U[r][c].imag();
+                    W[2 * c][2 * r + 1] = U[r][c].imag();
+                    W[2 * c + 1][2 * r + 1] = U[r][c].real();
+                }
+            TcBlock tb{};
+            for (int j = 0; j < 5; ++j) tb.k[j] = local_pos(gbit[j], st.pass.h);
+            int nr = 0;
+            for (int l = 0; l < kTcT; ++l) {
+                bool inb = false;
+                for (int j = 0; j < 5; ++j) inb |= tb.k[j] == l;
+                if (!inb) tb.row_bits[nr++] = l;
+            }
+            tb.b_offset = bimg.size();
+            bimg.resize(bimg.size() + 2 * kBBytes);
+            write_b_image(W, bimg.data() + tb.b_offset, bimg.data() + tb.b_offset + kBBytes);
+            blocks.push_back(tb);
+        }
+        step_pass[si] = (int)passes.size();
+        passes.push_back(tp);
+    }
+    const size_t bsz = blocks.size() * sizeof(TcBlock);
+    auto al = [](size_t x) { return (x + 1023) / 1024 * 1024; };
+    LQ_TRY(ensure_prog(s, al(bsz) + al(bimg.size()) + 1024));
+    TcBlock *d_blocks = (TcBlock *)s->d_prog;
+    unsigned char *d_bimg = (unsigned char *)s->d_prog + al(bsz);
+    LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (bsz) LQ_CUDA_TRY(cudaMemcpy(d_blocks, blocks.data(), bsz, cudaMemcpyHostToDevice));
+    if (!bimg.empty())
+        LQ_CUDA_TRY(cudaMemcpy(d_bimg, bimg.data(), bimg.size(), cudaMemcpyHostToDevice));
+    static bool attr = false;
+    if (!attr) {
+        LQ_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmem));
+        attr = true;
+    }
+    int launches = 0;
+    for (size_t si = 0; si < steps.size(); ++si) {
+        const PlanStep &st = steps[si];
+        if (!st.fused) {
+            LQ_TRY(launch_gate_op(s, gops[st.gate]));
+            continue;
+        }
+        const TcPass &tp = passes[step_pass[si]];
+        CUtensorMap map;
+        LQ_TRY(tc_tile_map(&map, s->d, n, tp.h));
+        prof_begin(s->stream, kProfTc);
+        k_tc_pass<<<1u << (n - kTcT), kTcThreads, kTcSmem, s->stream>>>(
+            map, tp.h, tp.h + 8, d_blocks + tp.block_begin, tp.nblocks, d_bimg, s->d_flag);
+        prof_end(s->stream, kProfTc);
+        LQ_CUDA_TRY(cudaGetLastError());
+        ++launches;
+    }
+    if (nblocks_out) *nblocks_out = (int)blocks.size();
+    if (npasses_out) *npasses_out = launches;
+    return LQ_OK;
+}
+
+}  // namespace lq
+
+using namespace lq;
+
+extern "C" {
+
+int lq_apply_circuit_tc(lq_state *s, int circuit_qubits, const lq_gate *ops, int nops,
+                        const double *theta, int ntheta, int *blocks, int *passes) {
+    LQ_TRY(check_state(s));
+    if (circuit_qubits != s->n)
+        return set_error(LQ_ERR_QUBIT_MISMATCH,
+                         "Circuit qubit count mismatch: circuit has %d, state has %d",
+                         circuit_qubits, s->n);
+    if (nops < 0 || (nops > 0 && !ops)) return set_error(LQ_ERR_INVALID_ARG, "bad op list");
+    if (ntheta < 0 || (ntheta > 0 && !theta)) return set_error(LQ_ERR_INVALID_ARG, "bad theta");
+    return apply_circuit_tc_impl(s, ops, nops, theta, ntheta, blocks, passes);
+}
+
+}  // extern "C"
