@@ -358,6 +358,47 @@ int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *e
  * lq_batch_gradients call for larger instances (0 before that call). */
 int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start.  No reference counterpart: the reference starts every
+ * VQE from caller-supplied angles (VQE::run, src/optimization/vqe.rs:69-88);
+ * these calls produce such angles.  A fully connected network in FP32 on the
+ * device: in_dim -> hidden (x depth, GELU) -> out_dim (linear).  Parameters are
+ * one flat vector, per layer W (out x in, row major) then b (out).
+ * ------------------------------------------------------------------------- */
+typedef struct lq_mlp lq_mlp;
+
+/* Seeded uniform He initialisation (last layer scaled by 0.1), zero biases. */
+int lq_mlp_create(int in_dim, int hidden, int depth, int out_dim, uint64_t seed, lq_mlp **out);
+int lq_mlp_destroy(lq_mlp *net);
+int lq_mlp_num_params(const lq_mlp *net, int64_t *out);
+int lq_mlp_get_params(const lq_mlp *net, float *host, int64_t count);
+int lq_mlp_set_params(lq_mlp *net, const float *host, int64_t count);
+/* Gradient of the last lq_mlp_loss_grad / lq_mlp_backward call. */
+int lq_mlp_get_grads(const lq_mlp *net, float *host, int64_t count);
+/* y[batch x out_dim] = net(x[batch x in_dim]); host buffers. */
+int lq_mlp_forward(lq_mlp *net, const float *x, int batch, float *y);
+/* Periodic angle loss  L = sum(mask * (1 - cos(y - target))) / sum(mask)  and
+ * dL/dparams (kept on the device for lq_mlp_adam_step). */
+int lq_mlp_loss_grad(lq_mlp *net, const float *x, const float *target, const float *mask,
+                     int batch, double *loss);
+/* dL/dparams for a caller-supplied dL/dy[batch x out_dim] (host) at inputs x:
+ * the chain rule through the network for any loss, e.g. the VQE energy with
+ * dE/dtheta from lq_batch_gradients. */
+int lq_mlp_backward(lq_mlp *net, const float *x, const float *dy, int batch);
+/* One Adam step on the device with the last gradient (bias-corrected, step
+ * count kept by the network). */
+int lq_mlp_adam_step(lq_mlp *net, float lr, float beta1, float beta2, float eps);
+/* Zero the Adam moments and step count (start of a new training stage). */
+int lq_mlp_reset_adam(lq_mlp *net);
+
+/* Exact ground energy of a real Pauli-sum Hamiltonian (every term with an even
+ * number of Y factors, as in the XYZ chains the VQE workloads use) by FP64
+ * Lanczos on the full 2^n space with full reorthogonalisation; stops when the
+ * lowest Ritz value moves by less than tol.  No reference counterpart (the
+ * reference has no exact solver); its energies are the yardstick for VQE. */
+int lq_lanczos_ground_energy(int num_qubits, const lq_pauli_term *terms, int nterms,
+                             int max_iter, double tol, uint64_t seed, double *e0, int *iters);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,19 @@ _PROTOS = {
     "lq_batch_num_params": (C.c_int, [_P, _PI]),
     "lq_batch_gradients": (C.c_int, [_P, _PD, C.c_double, _PD, _PD]),
     "lq_batch_tuning": (C.c_int, [_P, _PI, _PI]),
+    "lq_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "lq_mlp_destroy": (C.c_int, [_P]),
+    "lq_mlp_num_params": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "lq_mlp_get_params": (C.c_int, [_P, _PF, C.c_int64]),
+    "lq_mlp_set_params": (C.c_int, [_P, _PF, C.c_int64]),
+    "lq_mlp_get_grads": (C.c_int, [_P, _PF, C.c_int64]),
+    "lq_mlp_forward": (C.c_int, [_P, _PF, C.c_int, _PF]),
+    "lq_mlp_loss_grad": (C.c_int, [_P, _PF, _PF, _PF, C.c_int, _PD]),
+    "lq_mlp_backward": (C.c_int, [_P, _PF, _PF, C.c_int]),
+    "lq_mlp_adam_step": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "lq_mlp_reset_adam": (C.c_int, [_P]),
+    "lq_lanczos_ground_energy": (C.c_int, [C.c_int, _PT, C.c_int, C.c_int, C.c_double, C.c_uint64,
+                                           _PD, _PI]),
 }
 
 

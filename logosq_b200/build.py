@@ -25,6 +25,7 @@ SOURCES = [
     "profile.cu",
     "batch.cu",
     "tc.cu",
+    "learned.cu",
 ]
 
 NVCC_FLAGS = [

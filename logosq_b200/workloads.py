@@ -150,6 +150,26 @@ def heisenberg_instances(count: int, seed: int, n_lo=10, n_hi=20, layers=4):
     return out
 
 
+def disordered_chains(count: int, seed: int, n_lo=12, n_hi=16, disorder=0.2, layers=4):
+    """Learned-form workload: disordered XYZ open chains.  Per chain, mean
+    couplings (Jx, Jy, Jz) ~ U[-1, 1] and a field h ~ U[-0.5, 0.5]; per bond,
+    J_b = J + disorder * U[-1, 1] for each axis; n ~ U{n_lo..n_hi}.  Records
+    have the heisenberg_instances() layout (theta: random angles U[-pi, pi])."""
+    rng = SplitMix64(seed)
+    out = []
+    for _ in range(count):
+        n = rng.randint(n_lo, n_hi)
+        mx, my, mz = (rng.uniform(-1.0, 1.0) for _ in range(3))
+        h = rng.uniform(-0.5, 0.5)
+        jx = [mx + disorder * rng.uniform(-1.0, 1.0) for _ in range(n - 1)]
+        jy = [my + disorder * rng.uniform(-1.0, 1.0) for _ in range(n - 1)]
+        jz = [mz + disorder * rng.uniform(-1.0, 1.0) for _ in range(n - 1)]
+        theta = np.array([rng.uniform(-math.pi, math.pi) for _ in range(2 * n * layers)])
+        out.append({"n": n, "jx": np.array(jx), "jy": np.array(jy), "jz": np.array(jz),
+                    "h": h, "theta": theta, "layers": layers})
+    return out
+
+
 def heisenberg_terms(n, jx, jy, jz, h) -> np.ndarray:
     """Packed Pauli terms of sum_b (Jx XX + Jy YY + Jz ZZ)_b + h sum_i Z_i."""
     terms = []

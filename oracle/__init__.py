@@ -20,7 +20,7 @@ import numpy as np
 from logosq_b200 import abi
 
 HERE = Path(__file__).resolve().parent
-SRC = HERE / "logosq_oracle.cpp"
+SRCS = [HERE / "logosq_oracle.cpp", HERE / "mlp_oracle.cpp"]
 BUILD = HERE / "_build"
 LIB = BUILD / "liblogosq_oracle.so"
 
@@ -30,9 +30,9 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-sha
 def build(force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     hdr = HERE.parent / "include" / "logosq_b200.h"
-    if force or not LIB.exists() or LIB.stat().st_mtime < max(SRC.stat().st_mtime,
-                                                                hdr.stat().st_mtime):
-        subprocess.run(["g++", *CXXFLAGS, str(SRC), "-o", str(LIB)], check=True)
+    newest = max([s.stat().st_mtime for s in SRCS] + [hdr.stat().st_mtime])
+    if force or not LIB.exists() or LIB.stat().st_mtime < newest:
+        subprocess.run(["g++", *CXXFLAGS, *map(str, SRCS), "-o", str(LIB)], check=True)
     return LIB
 
 
@@ -45,6 +45,7 @@ def lib():
         build()
         lb = C.CDLL(str(LIB))
         PD, PG, PT = C.POINTER(C.c_double), C.POINTER(abi.LqGate), C.POINTER(abi.LqPauliTerm)
+        PF = C.POINTER(C.c_float)
         sig = {
             "or_set_threads": (None, [C.c_int]),
             "or_get_threads": (C.c_int, []),
@@ -67,6 +68,9 @@ def lib():
             "or_vqe_adam": (C.c_int, [C.c_int, PG, C.c_int, PD, C.c_int, PT, C.c_int, C.c_int,
                                       C.c_double, C.c_int, C.c_double, PD, PD]),
             "or_apply_dense": (None, [PD, C.c_int, PD]),
+            "or_mlp_num_params": (C.c_int64, [C.c_int] * 4),
+            "or_mlp_forward": (None, [C.c_int] * 4 + [PF, PF, C.c_int, PD]),
+            "or_mlp_loss_grad": (C.c_double, [C.c_int] * 4 + [PD, PF, PF, PF, C.c_int, PD]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lb, name)
@@ -175,3 +179,55 @@ def apply_dense(psi, matrix):
     lib().or_apply_dense(_pd(psi.view(np.float64)), int(np.log2(len(psi))),
                          _pd(m.view(np.float64)))
     return psi
+
+
+def _pf(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def mlp_num_params(in_dim, hidden, depth, out_dim) -> int:
+    return int(lib().or_mlp_num_params(in_dim, hidden, depth, out_dim))
+
+
+def mlp_forward(shape, params, x):
+    """FP64 forward pass of the warm-start network (mlp_oracle.cpp) for float32
+    parameters and inputs."""
+    in_dim, hidden, depth, out_dim = shape
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.zeros((len(xx), out_dim))
+    lib().or_mlp_forward(in_dim, hidden, depth, out_dim, _pf(p), _pf(xx), len(xx), _pd(y))
+    return y
+
+
+def mlp_loss_grad(shape, params, x, target, mask):
+    """FP64 periodic angle loss and its gradient w.r.t. the flat parameters."""
+    in_dim, hidden, depth, out_dim = shape
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    m = np.ascontiguousarray(mask, dtype=np.float32)
+    g = np.zeros(len(p))
+    loss = lib().or_mlp_loss_grad(in_dim, hidden, depth, out_dim, _pd(p), _pf(xx), _pf(t),
+                                  _pf(m), len(xx), _pd(g))
+    return loss, g
+
+
+def dense_hamiltonian(n: int, terms: np.ndarray) -> np.ndarray:
+    """Real dense matrix of a Pauli sum whose terms all carry an even number of
+    Y factors (textbook Pauli matrices; for such terms the reference's Y sign
+    convention gives the same operator).  Qubit q is bit n-1-q."""
+    N = 1 << n
+    idx = np.arange(N, dtype=np.int64)
+    H = np.zeros((N, N))
+    for t in terms:
+        x, z, ny = int(t["xmask"]), int(t["zmask"]), int(t["ny"])
+        assert ny % 2 == 0, "real Hamiltonian needs an even number of Y per term"
+        parity = np.zeros(N, dtype=np.int64)
+        zz = idx & z
+        while zz.any():
+            parity ^= zz & 1
+            zz >>= 1
+        phase = -1.0 if ny % 4 == 2 else 1.0
+        H[idx ^ x, idx] += float(t["coefficient"]) * phase * (1.0 - 2.0 * parity)
+    return H
