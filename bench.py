@@ -36,6 +36,7 @@ sys.path.insert(0, str(ROOT))
 
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM = 6650.0  # GB/s, earlier measurement on this pool
+FP64_PEAK_TFLOPS = 36.6  # dependent-chain-free DFMA throughput measured on this pool's B200
 
 
 def hbm_peak():
@@ -144,7 +145,8 @@ def run_vqe_batch(args):
     from logosq_b200._lib import call
     from logosq_b200.batch import heisenberg_batch
 
-    recs = workloads.heisenberg_instances(args.instances, seed=4, n_lo=10, n_hi=20)
+    lo, hi = args.n_lo or 10, args.n_hi or 20
+    recs = workloads.heisenberg_instances(args.instances, seed=4, n_lo=lo, n_hi=hi)
     theta = np.concatenate([r["theta"] for r in recs])
     total_params = len(theta)
     t0 = time.perf_counter()
@@ -186,13 +188,13 @@ def run_vqe_batch(args):
         st.close()
     plain_s = sum(plain_time[r["n"]] for r in recs)
     tune = b.tuning()
-    line = {"metric": "batched VQE gradients/s (256 XYZ chains, n 10-20, L=4)",
+    line = {"metric": f"batched VQE gradients/s ({len(recs)} XYZ chains, n {lo}-{hi}, L=4)",
             "value": total_params / batched_s, "unit": "gradients/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (complex128)", "data": "synthetic (seeded)",
             "config": {"workload": "batching form", "instances": len(recs),
-                       "qubits": "10-20", "total_params": total_params,
+                       "qubits": f"{lo}-{hi}", "total_params": total_params,
                        "circuits": int(sum(2 * 8 * r["n"] + 1 for r in recs)),
                        "autotuned_tile_bits": tune["tile_bits"],
                        "smem_resident_max_qubits": tune["smem_max_qubits"]},
@@ -270,8 +272,24 @@ def run_precision(args):
     # 3xTF32: 3 real 128x64x64 GEMMs per 128 rows of 32 amplitudes
     flops_per_block = 3 * 2 * 64 * 64 * (1 << n) // 32 * 2
     st32.close()
-    # 30-qubit comparison against the complex128 engine
-    m = 30
+    line = {"metric": f"precision form {n}q complex64 gate-layer GB/s (tcgen05 3xTF32 blocks)",
+            "value": workloads.brickwork_bytes(n, 20, amp_bytes=8) / (ms / 1e3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "tf32x3 -> f32 (complex64)",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"U3+CNOT brickwork, {n} qubits complex64, 20 layers, seed 3",
+                       "blocks_per_step": nblocks, "passes_per_step": npasses},
+            "roofline": {"kernel": "k_tc_pass", "bound": "hbm", "avg_launch_ms": launch_ms,
+                         "achieved": 2 * S / (launch_ms / 1e3) / 1e9, "unit": "GB/s",
+                         "peak": hbm_peak()[0],
+                         "frac": 2 * S / (launch_ms / 1e3) / 1e9 / hbm_peak()[0],
+                         "tensor_tflops_issued": flops_per_block * nblocks / (ms / 1e3) / 1e12},
+            "fp64_norm": norm32, "fp64_zstring_energy": e32}
+    if args.check_qubits <= 0:
+        print(json.dumps(line), flush=True)
+        return 0
+    # comparison against the complex128 engine on the same circuit
+    m = args.check_qubits
     st64, g30, _, _, _, _ = run_tc(m, 20, 1, 0)
     ref = State.zero_state(m)
     call("lq_apply_circuit", ref.handle, m, abi.gate_ptr(g30), len(g30), None, 0, abi.EXEC_FUSED)
@@ -290,23 +308,134 @@ def run_precision(args):
     amp_scale = float(b.abs().max().item())
     e30_tc, e30_ref = zz_energy(st64, m), zz_energy(ref, m)
     norm30 = st64.norm_sqr()
-    line = {"metric": f"precision form {n}q complex64 gate-layer GB/s (tcgen05 3xTF32 blocks)",
-            "value": workloads.brickwork_bytes(n, 20, amp_bytes=8) / (ms / 1e3) / 1e9,
-            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "dtype": "tf32x3 -> f32 (complex64)",
-            "data": "synthetic (seeded)",
-            "config": {"workload": f"U3+CNOT brickwork, {n} qubits complex64, 20 layers, seed 3",
-                       "blocks_per_step": nblocks, "passes_per_step": npasses},
-            "roofline": {"kernel": "k_tc_pass", "bound": "hbm", "avg_launch_ms": launch_ms,
-                         "achieved": 2 * S / (launch_ms / 1e3) / 1e9, "unit": "GB/s",
-                         "peak": hbm_peak()[0],
-                         "frac": 2 * S / (launch_ms / 1e3) / 1e9 / hbm_peak()[0],
-                         "tensor_tflops_issued": flops_per_block * nblocks / (ms / 1e3) / 1e12},
-            "fp64_norm": norm32, "fp64_zstring_energy": e32,
-            "check_30q": {"max_abs_amplitude_error": maxabs, "max_abs_amplitude": amp_scale,
-                          "zstring_energy_tc": e30_tc, "zstring_energy_c128": e30_ref,
-                          "energy_abs_error": abs(e30_tc - e30_ref), "fp64_norm_tc": norm30}}
+    line[f"check_{m}q"] = {"max_abs_amplitude_error": maxabs, "max_abs_amplitude": amp_scale,
+                           "zstring_energy_tc": e30_tc, "zstring_energy_c128": e30_ref,
+                           "energy_abs_error": abs(e30_tc - e30_ref), "fp64_norm_tc": norm30}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_learned(args):
+    """Learned form: disordered XYZ chains (n 12-16 by default).  Train the
+    warm-start network on batched-VQE optima (fixed small-angle start), then on
+    the simulator's energy; evaluate on fresh chains: iterations and wall time
+    to reach E* + 1e-3 (E* = the lowest energy any start reached) for
+    warm-started batched VQE vs random-init VQE, batched and on the plain
+    per-circuit path; exact E0 from the FP64 Lanczos."""
+    from logosq_b200 import State, abi, learned, workloads
+    from logosq_b200._lib import call
+
+    lo, hi = args.n_lo or 12, args.n_hi or 16
+    t0 = time.perf_counter()
+    train = workloads.disordered_chains(args.train_chains, seed=5, n_lo=lo, n_hi=hi)
+    X, T, M, _, data_sec = learned.optimum_dataset(train, iters=args.vqe_iters)
+    t_data = time.perf_counter() - t0
+    net = learned.WarmStartMLP(seed=1)
+    t0 = time.perf_counter()
+    hist = net.fit(X, T, M, epochs=args.epochs, batch=256, lr=1e-3, val_frac=0.1)
+    t_fit = time.perf_counter() - t0
+    p_sup = net.params()
+    t0 = time.perf_counter()
+    eh = net.energy_train(train, args.energy_steps, lr=3e-4)
+    t_energy = time.perf_counter() - t0
+
+    ev = workloads.disordered_chains(args.eval_chains, seed=6, n_lo=lo, n_hi=hi)
+    Xe = np.stack([learned.features(r) for r in ev])
+    net.forward(Xe)
+    t0 = time.perf_counter()
+    Yw = net.forward(Xe)
+    t_infer = time.perf_counter() - t0
+    warm = [Yw[i, :8 * r["n"]].astype(np.float64) for i, r in enumerate(ev)]
+    p_full = net.params()
+    net.set_params(p_sup)
+    sup = net.warm_start(ev)
+    net.set_params(p_full)
+    rng = np.random.default_rng(6)
+    starts = {"random": [learned.random_start(r["n"], rng) for r in ev],
+              "fixed_small_angle": [learned.fixed_start(r["n"]) for r in ev],
+              "supervised_only": sup, "warm": warm}
+    iters = args.eval_iters
+    traces, sec = {}, {}
+    for k, st in starts.items():
+        _, traces[k], sec[k] = learned.batched_vqe(ev, st, iters)
+    t0 = time.perf_counter()
+    E0 = np.array([learned.lanczos_ground_energy(r["n"], learned.chain_terms(r))[0] for r in ev])
+    t_lanczos = time.perf_counter() - t0
+    best = np.min([tr.min(axis=1) for tr in traces.values()], axis=0)
+    tol = 1e-3
+    its = {k: learned.iterations_to(tr, best, tol) for k, tr in traces.items()}
+    cap = iters + 1
+
+    # plain per-circuit path (the reference's VQE loop shape): one energy and one
+    # parameter-shift gradient per iteration, timed once per qubit count
+    t_plain = {}
+    for n in sorted({r["n"] for r in ev}):
+        i = next(j for j, x in enumerate(ev) if x["n"] == n)
+        gates = workloads.basic_entangling_template(n, 4)
+        terms = learned.chain_terms(ev[i])
+        th = np.ascontiguousarray(starts["random"][i])
+        gp = np.zeros(len(th))
+        e = C.c_double()
+        st = State.zero_state(n)
+        common = (st.handle, abi.gate_ptr(gates), len(gates), abi.f64_ptr(th), len(th),
+                  abi.term_ptr(terms), len(terms), abi.Y_REFERENCE)
+        for _ in range(2):  # the first call warms up
+            tt = time.perf_counter()
+            call("lq_ansatz_energy", *common, C.byref(e))
+            call("lq_parameter_shift", *common, math.pi / 2, abi.f64_ptr(gp))
+            t_plain[n] = time.perf_counter() - tt
+        st.close()
+
+    def batched_wall(k):
+        tot = 0.0
+        for ci, c0 in enumerate(range(0, len(ev), 256)):
+            tot += min(int(its[k][c0:c0 + 256].max()), cap) * sec[k][ci]
+        return tot
+
+    plain_random = float(sum(min(int(i), cap) * t_plain[r["n"]]
+                             for i, r in zip(its["random"], ev)))
+    warm_batched = t_infer + batched_wall("warm")
+    summary = {}
+    for k in traces:
+        summary[k] = {"median_iters_to_target": float(np.median(its[k])),
+                      "reached_target_frac": float(np.mean(its[k] < cap)),
+                      "median_initial_gap_to_best": float(np.median(traces[k][:, 0] - best)),
+                      "median_final_gap_to_E0": float(np.median(traces[k][:, -1] - E0)),
+                      "batched_wall_s_to_target": batched_wall(k),
+                      "batched_s_per_iteration": sec[k]}
+    line = {"metric": "learned warm start: wall-seconds to E*+1e-3, plain per-circuit "
+                      "random-init VQE / warm-started batched VQE",
+            "value": plain_random / warm_batched, "unit": "x", "n_gpus": 1,
+            "steps": iters, "warmup": 1, "ms_per_step": sec["warm"][0] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 simulator, f32 network", "data": "synthetic (seeded)",
+            "config": {"workload": f"disordered XYZ chains n {lo}-{hi} (mean J ~ U[-1,1], "
+                                   "+-0.2 per-bond disorder, h ~ U[-0.5,0.5]), BasicEntangling "
+                                   "L=4, Adam lr 0.05",
+                       "train_chains": len(train), "train_vqe_iters": args.vqe_iters,
+                       "supervised_epochs": args.epochs, "energy_steps": args.energy_steps,
+                       "eval_chains": len(ev), "eval_iters": iters, "target_tol": tol,
+                       "wall_model": "iterations to target x measured seconds per iteration; "
+                                     "a chunk of 256 chains runs until its slowest chain "
+                                     "reaches the target (cap = eval_iters + 1)"},
+            "plain_random_wall_s_to_target": plain_random,
+            "warm_batched_wall_s_to_target": warm_batched,
+            "batched_random_wall_s_to_target": batched_wall("random"),
+            "plain_s_per_iteration_by_qubits": t_plain,
+            "starts": summary,
+            "exact": {"min_gap_best_to_E0": float((best - E0).min()),
+                      "median_gap_best_to_E0": float(np.median(best - E0)),
+                      "frac_within_1e-3_of_E0": float(np.mean(best - E0 < 1e-3)),
+                      "lanczos_s": t_lanczos},
+            "training": {"dataset_s": t_data, "dataset_s_per_iteration": data_sec,
+                         "supervised_fit_s": t_fit,
+                         "supervised_loss_first_last": [hist[0], hist[-1]],
+                         "heldout_loss_best": float(min(net.val_hist)) if net.val_hist else None,
+                         "energy_stage_s": t_energy,
+                         "energy_stage_mean_E_first_last": [eh[0], eh[-1]],
+                         "inference_s": t_infer}}
+    print(json.dumps(line), flush=True)
+    net.close()
     return 0
 
 
@@ -331,13 +460,28 @@ def main():
     ap.add_argument("--fusion-width", type=int, default=0,
                     help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
     ap.add_argument("--workload", default="brickwork",
-                    choices=["brickwork", "vqe-batch", "precision"])
+                    choices=["brickwork", "vqe-batch", "precision", "learned"])
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--check-qubits", type=int, default=30,
+                    help="precision form: qubit count of the comparison against complex128 "
+                         "(0 = skip)")
+    ap.add_argument("--train-chains", type=int, default=1024)
+    ap.add_argument("--vqe-iters", type=int, default=150)
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--energy-steps", type=int, default=300)
+    ap.add_argument("--eval-chains", type=int, default=256)
+    ap.add_argument("--eval-iters", type=int, default=300)
+    ap.add_argument("--n-lo", type=int, default=None,
+                    help="smallest chain (vqe-batch: 10, learned: 12)")
+    ap.add_argument("--n-hi", type=int, default=None,
+                    help="largest chain (vqe-batch: 20, learned: 16)")
     args = ap.parse_args()
     if args.workload == "vqe-batch":
         return run_vqe_batch(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "learned":
+        return run_learned(args)
     n, layers = args.qubits, args.layers
     ws, rank, local = dist_info()
     metric = f"{n}q gate-layer GB/s"
@@ -446,12 +590,25 @@ def main():
     peak, peak_kind = hbm_peak()
     fused_launch_ms = fused_ms.value / max(fused_n.value, 1)
     achieved = 2 * S / (fused_launch_ms / 1e3) / 1e9 if fused_n.value else None
-    roofline = {"kernel": "k_fused_pass (TMA-staged 2^12-amplitude tiles)", "bound": "hbm",
+    # ncu (profiles/k_fused_pass_brickwork26q.md): dram read + write per launch at 26
+    # qubits = 2.096e9 B (0.976 x 2S); a launch sweeps the whole state, so scale by 2^(n-26).
+    traffic = 2.096e9 * 2.0 ** (n - 26)
+    n_u3 = int(np.sum(gates["kind"] == abi.U3))
+    fp64_flops_step = 14.0 * n_u3 * (1 << n)  # 2x2 complex matrix: 14 flops per amplitude
+    roofline = {"kernel": "k_fused_pass (TMA-staged 2^T-amplitude tiles)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": 2 * S, "avg_launch_ms": fused_launch_ms,
                 "launches_per_step": passes.value,
-                "traffic": None, "traffic_note": "see profiles/ (ncu dram bytes per launch)"}
+                "traffic": traffic,
+                "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                "captured at 26 qubits and scaled by 2^(n-26)",
+                "fp64": {"achieved_tflops": fp64_flops_step / (ms_step / 1e3) / 1e12,
+                         "peak_tflops": FP64_PEAK_TFLOPS,
+                         "frac": fp64_flops_step / (ms_step / 1e3) / 1e12 / FP64_PEAK_TFLOPS,
+                         "peak_source": "DFMA throughput probe on this pool's B200",
+                         "flops_per_step": fp64_flops_step,
+                         "note": "the fused kernel is FP64 / issue bound (profiles/)"}}
 
     # ---- per-gate (unfused) path: one sweep per gate, as Gate::apply --------
     per_gate = None
