@@ -145,10 +145,17 @@ def run_vqe_batch(args):
     from logosq_b200._lib import call
     from logosq_b200.batch import heisenberg_batch
 
+    from logosq_b200 import replicas
     lo, hi = args.n_lo or 10, args.n_hi or 20
-    recs = workloads.heisenberg_instances(args.instances, seed=4, n_lo=lo, n_hi=hi)
+    all_recs = workloads.heisenberg_instances(args.instances, seed=4, n_lo=lo, n_hi=hi)
+    ws, rank, local = replicas.dist_info()
+    torch.cuda.set_device(local)
+    if ws > 1:  # instances are independent: each rank takes a cost-balanced share
+        replicas.init("nccl", timeout_s=300)
+    costs = [replicas.instance_cost(r["n"], 8 * r["n"]) for r in all_recs]
+    recs = [all_recs[i] for i in replicas.shard_instances(costs, ws, rank)]
     theta = np.concatenate([r["theta"] for r in recs])
-    total_params = len(theta)
+    total_params = sum(8 * r["n"] for r in all_recs)
     t0 = time.perf_counter()
     b = heisenberg_batch(recs)
     create_s = time.perf_counter() - t0
@@ -158,10 +165,11 @@ def run_vqe_batch(args):
     for _ in range(max(args.warmup - 1, 0)):
         b.gradients(theta)
     torch.cuda.synchronize()
+    replicas.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e, g = b.gradients(theta)
-    batched_s = (time.perf_counter() - t0) / args.steps
+        e, g = b.gradients(theta)  # returns after the device finished the step
+    batched_s = replicas.max_over_ranks((time.perf_counter() - t0) / args.steps)
     # plain per-circuit path on one instance per qubit count
     sample = {}
     for i, r in enumerate(recs):
@@ -186,16 +194,19 @@ def run_vqe_batch(args):
         plain_time[n] = time.perf_counter() - t0
         max_err = max(max_err, float(np.abs(gp - gs[i]).max()))
         st.close()
-    plain_s = sum(plain_time[r["n"]] for r in recs)
+    plain_s = replicas.max_over_ranks(sum(plain_time[r["n"]] for r in recs))
+    max_err = replicas.max_over_ranks(max_err)
     tune = b.tuning()
-    line = {"metric": f"batched VQE gradients/s ({len(recs)} XYZ chains, n {lo}-{hi}, L=4)",
-            "value": total_params / batched_s, "unit": "gradients/s", "n_gpus": 1,
+    line = {"metric": f"batched VQE gradients/s ({len(all_recs)} XYZ chains, n {lo}-{hi}, L=4)",
+            "value": total_params / batched_s, "unit": "gradients/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (complex128)", "data": "synthetic (seeded)",
-            "config": {"workload": "batching form", "instances": len(recs),
+            "config": {"workload": "batching form", "instances": len(all_recs),
                        "qubits": f"{lo}-{hi}", "total_params": total_params,
-                       "circuits": int(sum(2 * 8 * r["n"] + 1 for r in recs)),
+                       "circuits": int(sum(2 * 8 * r["n"] + 1 for r in all_recs)),
+                       "parallelism": f"instances sharded over {ws} ranks" if ws > 1
+                       else "single GPU",
                        "autotuned_tile_bits": tune["tile_bits"],
                        "smem_resident_max_qubits": tune["smem_max_qubits"]},
             "plain_per_circuit": {"value": total_params / plain_s, "unit": "gradients/s",
@@ -204,8 +215,11 @@ def run_vqe_batch(args):
             "speedup_vs_plain": plain_s / batched_s,
             "max_abs_gradient_diff_vs_plain": max_err,
             "first_call_s": first_s, "create_s": create_s}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     b.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
     return 0
 
 
@@ -440,10 +454,8 @@ def run_learned(args):
 
 
 def dist_info():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from logosq_b200.replicas import dist_info as di
+    return di()
 
 
 def main():
@@ -510,13 +522,12 @@ def main():
         return 0
 
     import torch
-    from logosq_b200 import State, abi, workloads
+    from logosq_b200 import State, abi, replicas, workloads
     from logosq_b200._lib import call, lib
 
-    if ws > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
+    if ws > 1:
+        replicas.init("nccl", timeout_s=300)
     call("lq_set_device", local)
 
     gates = workloads.brickwork_u3(n, layers, seed=2)
@@ -560,8 +571,7 @@ def main():
 
     # ---- timed region (device time, CUDA events on the engine's stream) ----
     call("lq_profile_enable", 1)
-    if ws > 1:
-        torch.distributed.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[local])
                            if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
@@ -580,12 +590,9 @@ def main():
     fused_ms, fused_n = C.c_double(), C.c_longlong()
     call("lq_profile_read", 0, C.byref(fused_ms), C.byref(fused_n))
     call("lq_profile_enable", 0)
-    if ws > 1:
-        t = torch.tensor([ms_total], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = replicas.max_over_ranks(ms_total)  # slowest replica
     ms_step = ms_total / args.steps
-    value = ws * algo_bytes / (ms_step / 1e3) / 1e9
+    value = replicas.job_throughput(algo_bytes, ms_step / 1e3, ws) / 1e9
 
     peak, peak_kind = hbm_peak()
     fused_launch_ms = fused_ms.value / max(fused_n.value, 1)
@@ -647,11 +654,8 @@ def main():
                  None, 0, abi.EXEC_FUSED)
             call("lq_state_download", st.handle, pinned_ptr, C.c_size_t(1 << n))
         dt = (time.perf_counter() - t0) / e2e_steps
-        if ws > 1:
-            t = torch.tensor([dt], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            dt = float(t.item())
-        e2e = {"value": ws * algo_bytes / dt / 1e9, "unit": "GB/s",
+        dt = replicas.max_over_ranks(dt)
+        e2e = {"value": replicas.job_throughput(algo_bytes, dt, ws) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(gates.nbytes), "d2h_bytes_per_step": int(S),
                "s_per_step": dt, "result": "final state vector downloaded to pinned host memory"}
         del pinned
