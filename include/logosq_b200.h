@@ -357,6 +357,10 @@ int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *e
  * and the fusion width (tile bits) the autotuner chose on the first
  * lq_batch_gradients call for larger instances (0 before that call). */
 int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits);
+/* Force the fusion width (tile bits 10, 11 or 12) of the instances larger than
+ * 2^12 amplitudes, or 0 to autotune again on the next lq_batch_gradients call.
+ * No reference counterpart (tuning control of this engine). */
+int lq_batch_set_tile_bits(lq_batch *b, int tile_bits);
 
 /* ---------------------------------------------------------------------------
  * Learned warm start.  No reference counterpart: the reference starts every

@@ -67,9 +67,12 @@ struct BProgram {  // device program for one fusion width
     BPass *passes = nullptr;
     BInst *insts = nullptr;
     std::vector<BInst> h_insts;
+    std::vector<FusedOp> h_ops;  // host copy of ops (parameter bindings)
     size_t ncoef = 0;
     // per instance: host copies needed to refresh coefficients
-    std::vector<std::vector<int>> op_gate;  // fop index (instance-local) -> gate index
+    // fop index (instance-local) -> the gates it applies, in order (more than one
+    // for a merged run of single-qubit gates on one qubit)
+    std::vector<std::vector<std::vector<int>>> op_members;
     std::vector<std::vector<PlanStep>> steps;
     std::vector<int> op_begin;  // first fop of each instance
     std::vector<int> nops;
@@ -229,13 +232,20 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         auto coef_of = [&](const FusedOp &op) {
             if (op.param >= 0 && op.param == cur_p)
                 return icoef + op.coef_alt + (minus ? (op.type == F_M2 ? 32 : 8) : 0);
+            if (op.param2 >= 0 && op.param2 == cur_p)
+                return icoef + op.coef_alt2 + (minus ? 8 : 0);
             return icoef + op.coef;
         };
         const int T = in.T;
         const int nthr = 1 << (T - 4);
         double acc = 0.0;
-        if (in.n <= kSmemStateMax) {
-            // whole state in shared memory: |0...0>
+        // n <= 12: the whole state is one tile in shared memory; otherwise it
+        // lives in this CTA's HBM slot and every pass sweeps it tile by tile.
+        // One code path for both keeps a single inlined copy of the register
+        // rounds (register pressure).  Only the 2^(T-4) threads that own
+        // amplitudes run a round.
+        const bool in_smem = in.n <= kSmemStateMax;
+        if (in_smem) {
             for (int l = tid; l < (1 << T); l += kBatchThreads) {
                 const double re = l == 0 ? 1.0 : 0.0;
                 asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(tile_a +
@@ -243,59 +253,56 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                              "d"(re), "d"(0.0)
                              : "memory");
             }
-            __syncthreads();
-            for (int p = 0; p < in.npass; ++p) {
-                const BPass ps = passes[in.pass_begin + p];
-                for (int r = 0; r < ps.nrounds; ++r) {
-                    if (tid < nthr)
-                        run_round<false>(tile_a, rounds[ps.round_begin + r], ops, coef_of, 0ull,
-                                         ps.h, tid);
-                    __syncthreads();
-                }
-            }
-            for (int w = 0; w < in.newin; ++w) {
-                const BEWin ew = ewins[in.ewin_begin + w];
-                acc += tile_energy(tile_a, T, ew.h, 0ull, groups, ew.group_begin, ew.ngroups,
-                                   terms, tid, kBatchThreads);
-            }
         } else {
-            // state in this CTA's HBM slot, swept in tiles
             const uint64_t N = 1ull << in.n;
             for (uint64_t i = tid; i < N; i += kBatchThreads)
                 slot[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
-            __syncthreads();
-            const int ntiles = 1 << (in.n - T);
-            for (int p = 0; p < in.npass; ++p) {
-                const BPass ps = passes[in.pass_begin + p];
-                const int h = ps.h, hm = ps.h + T - 4;
-                for (int t = 0; t < ntiles; ++t) {
-                    const uint64_t c2 = (uint64_t)(t & ((1 << (h - 4)) - 1));
-                    const uint64_t c4 = (uint64_t)(t >> (h - 4));
-                    const uint64_t tb = (c2 << 4) | (c4 << hm);
-                    gather_tile(tile_a, slot, T, h, tb, tid);
+        }
+        __syncthreads();
+        const int ntiles = in_smem ? 1 : 1 << (in.n - T);
+        auto tile_base = [&](int t, int h) -> uint64_t {
+            if (in_smem) return 0ull;
+            const uint64_t c2 = (uint64_t)(t & ((1 << (h - 4)) - 1));
+            const uint64_t c4 = (uint64_t)(t >> (h - 4));
+            return (c2 << 4) | (c4 << (h + T - 4));
+        };
+        for (int p = 0; p < in.npass; ++p) {
+            const BPass ps = passes[in.pass_begin + p];
+            for (int t = 0; t < ntiles; ++t) {
+                const uint64_t tb = tile_base(t, ps.h);
+                if (!in_smem) {
+                    gather_tile(tile_a, slot, T, ps.h, tb, tid);
                     __syncthreads();
-                    for (int r = 0; r < ps.nrounds; ++r) {
-                        run_round<false>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb, h,
-                                         tid);
-                        __syncthreads();
-                    }
-                    scatter_tile(tile_a, slot, T, h, tb, tid);
+                }
+                for (int r = 0; r < ps.nrounds; ++r) {
+                    // A branch around the round costs the full-width case (all 256
+                    // threads own amplitudes) much of its speed: give it its own
+                    // unconditional copy.
+                    if (nthr == kBatchThreads)
+                        run_round<0>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb,
+                                     ps.h, tid);
+                    else if (tid < nthr)
+                        run_round<0>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb,
+                                     ps.h, tid);
+                    __syncthreads();
+                }
+                if (!in_smem) {
+                    scatter_tile(tile_a, slot, T, ps.h, tb, tid);
                     __syncthreads();
                 }
             }
-            for (int w = 0; w < in.newin; ++w) {
-                const BEWin ew = ewins[in.ewin_begin + w];
-                const int h = ew.h, hm = ew.h + T - 4;
-                for (int t = 0; t < ntiles; ++t) {
-                    const uint64_t c2 = (uint64_t)(t & ((1 << (h - 4)) - 1));
-                    const uint64_t c4 = (uint64_t)(t >> (h - 4));
-                    const uint64_t tb = (c2 << 4) | (c4 << hm);
-                    gather_tile(tile_a, slot, T, h, tb, tid);
-                    __syncthreads();
-                    acc += tile_energy(tile_a, T, h, tb, groups, ew.group_begin, ew.ngroups,
-                                       terms, tid, kBatchThreads);
+        }
+        for (int w = 0; w < in.newin; ++w) {
+            const BEWin ew = ewins[in.ewin_begin + w];
+            for (int t = 0; t < ntiles; ++t) {
+                const uint64_t tb = tile_base(t, ew.h);
+                if (!in_smem) {
+                    gather_tile(tile_a, slot, T, ew.h, tb, tid);
                     __syncthreads();
                 }
+                acc += tile_energy(tile_a, T, ew.h, tb, groups, ew.group_begin, ew.ngroups, terms,
+                                   tid, kBatchThreads);
+                if (!in_smem) __syncthreads();  // before the next gather overwrites the tile
             }
         }
         // block reduction of the FP64 energy (fixed order)
@@ -314,6 +321,158 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
 
 static size_t batch_smem() { return (16u << kMaxT) + 2048; }
 
+// 2x2 matrix (m00, m01, m10, m11 as re/im pairs) of an uncontrolled
+// single-qubit op and the index bit it acts on; false for any other op.
+static bool single_bit_matrix(const GateOp &g, int &bit, double m[8]) {
+    if (g.renorm) return false;
+    if ((g.type == OP_M1 || g.type == OP_PERM1) && g.nctrl == 0) {
+        bit = g.t;
+        if (g.type == OP_M1) {
+            for (int q = 0; q < 8; ++q) m[q] = g.m[q];
+        } else {
+            const double x[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+            for (int q = 0; q < 8; ++q) m[q] = x[q];
+        }
+        return true;
+    }
+    if (g.type == OP_DIAG && g.nfix == 0 && g.npat == 1) {
+        bit = g.pat[0];
+        const double d[8] = {g.m[0], g.m[1], 0, 0, 0, 0, g.m[2], g.m[3]};
+        for (int q = 0; q < 8; ++q) m[q] = d[q];
+        return true;
+    }
+    return false;
+}
+
+// out = b . a (2x2 complex, re/im pairs): a is applied first.
+static void mat2_mul(const double b[8], const double a[8], double out[8]) {
+    for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 2; ++c) {
+            double re = 0.0, im = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                const double br = b[(r * 2 + k) * 2], bi = b[(r * 2 + k) * 2 + 1];
+                const double ar = a[(k * 2 + c) * 2], ai = a[(k * 2 + c) * 2 + 1];
+                re += br * ar - bi * ai;
+                im += br * ai + bi * ar;
+            }
+            out[(r * 2 + c) * 2] = re;
+            out[(r * 2 + c) * 2 + 1] = im;
+        }
+}
+
+// The parameter a gate is bound to (-1: none); LQ_ERR_UNSUPPORTED for two.
+static int gate_param(const lq_gate &g, int *p) {
+    *p = -1;
+    for (int a = 0; a < 3; ++a)
+        if (g.param[a] >= 0) {
+            if (*p >= 0 && g.param[a] != *p)
+                return set_error(LQ_ERR_UNSUPPORTED,
+                                 "batched engine: a gate bound to two parameters");
+            *p = g.param[a];
+        }
+    return LQ_OK;
+}
+
+// Coefficients of one encoded op for angles tp: a single gate's own (8 or 32
+// doubles, zeros for pure permutations), or the product of a merged run of
+// single-qubit gates (8 doubles: a 2x2 for F_M1, phases (d0, d1) for F_DIAG).
+static int op_coefficients(const std::vector<lq_gate> &gates, const std::vector<int> &members,
+                           const double *tp, int n, double *out) {
+    if (members.size() == 1) {
+        GateOp op;
+        LQ_TRY(make_gate_op(&gates[members[0]], tp, n, &op));
+        const int nc = op.type == OP_M2 ? 32 : 8;
+        for (int q = 0; q < nc; ++q)
+            out[q] = (op.type == OP_PERM1 || op.type == OP_SWAP) ? 0.0 : op.m[q];
+        return LQ_OK;
+    }
+    double acc[8] = {1, 0, 0, 0, 0, 0, 1, 0}, m[8], t[8];
+    bool diag = true;
+    for (int k : members) {
+        GateOp op;
+        LQ_TRY(make_gate_op(&gates[k], tp, n, &op));
+        int bit;
+        if (!single_bit_matrix(op, bit, m))
+            return set_error(LQ_ERR_INVALID_ARG, "batched engine: bad merged gate");
+        diag = diag && op.type == OP_DIAG;
+        mat2_mul(m, acc, t);
+        for (int q = 0; q < 8; ++q) acc[q] = t[q];
+    }
+    if (diag) {
+        const double d[8] = {acc[0], acc[1], acc[6], acc[7], 0, 0, 0, 0};
+        for (int q = 0; q < 8; ++q) out[q] = d[q];
+    } else {
+        for (int q = 0; q < 8; ++q) out[q] = acc[q];
+    }
+    return LQ_OK;
+}
+
+// Merge runs of uncontrolled single-qubit gates on the same qubit (no gate in
+// between touches that qubit, so the run commutes into one place) into one op,
+// as long as the run is bound to at most two parameters.  Returns the ops to
+// plan and, per op, the gates it applies.
+static int merge_single_qubit_runs(const std::vector<lq_gate> &gates, int n,
+                                   std::vector<GateOp> &mops,
+                                   std::vector<std::vector<int>> &members) {
+    int maxp = 0;
+    for (const auto &gt : gates)
+        for (int a = 0; a < 3; ++a) maxp = std::max(maxp, gt.param[a] + 1);
+    std::vector<double> zeros(maxp + 1, 0.0);
+    std::vector<int> open(64, -1);   // per index bit: op a single-qubit gate may join
+    std::vector<int> run_params;     // per op: distinct bound parameters (2 slots)
+    std::vector<char> all_diag;
+    mops.clear();
+    members.clear();
+    for (size_t k = 0; k < gates.size(); ++k) {
+        GateOp g;
+        LQ_TRY(make_gate_op(&gates[k], zeros.data(), n, &g));
+        int p;
+        LQ_TRY(gate_param(gates[k], &p));
+        int bit = -1;
+        double m[8];
+        const bool single = single_bit_matrix(g, bit, m);
+        if (single && open[bit] >= 0) {
+            const int e = open[bit];
+            int &p0 = run_params[2 * e], &p1 = run_params[2 * e + 1];
+            const bool fits = p < 0 || p == p0 || p == p1 || p0 < 0 || p1 < 0;
+            if (fits) {
+                if (p >= 0 && p != p0 && p != p1) (p0 < 0 ? p0 : p1) = p;
+                members[e].push_back((int)k);
+                all_diag[e] = all_diag[e] && g.type == OP_DIAG;
+                continue;
+            }
+        }
+        const uint64_t bits = op_bits(g);
+        for (int b = 0; b < 64; ++b)
+            if ((bits >> b) & 1) open[b] = -1;
+        mops.push_back(g);
+        members.push_back({(int)k});
+        run_params.push_back(p);
+        run_params.push_back(-1);
+        all_diag.push_back(g.type == OP_DIAG);
+        if (single) open[bit] = (int)mops.size() - 1;
+    }
+    // merged runs become one 2x2 (or one diagonal) op on their qubit
+    for (size_t e = 0; e < mops.size(); ++e) {
+        if (members[e].size() == 1) continue;
+        int bit;
+        double m[8];
+        single_bit_matrix(mops[e], bit, m);
+        GateOp g;
+        if (all_diag[e]) {
+            g.type = OP_DIAG;
+            g.npat = 1;
+            g.pat[0] = bit;
+        } else {
+            g.type = OP_M1;
+            g.t = bit;
+        }
+        LQ_TRY(op_coefficients(gates, members[e], zeros.data(), n, g.m));
+        mops[e] = g;
+    }
+    return LQ_OK;
+}
+
 // Build the device program of every instance for fusion width Tw.
 static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     pg.T = Tw;
@@ -322,7 +481,7 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     std::vector<BPass> passes;
     std::vector<double> dummy;
     pg.h_insts.clear();
-    pg.op_gate.assign(b->ninst, {});
+    pg.op_members.assign(b->ninst, {});
     pg.steps.assign(b->ninst, {});
     pg.op_begin.assign(b->ninst, 0);
     pg.nops.assign(b->ninst, 0);
@@ -330,10 +489,9 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     for (int i = 0; i < b->ninst; ++i) {
         const int n = b->n[i];
         const int T = n <= kSmemStateMax ? n : std::min(Tw, n);
-        std::vector<GateOp> gops(b->ops[i].size());
-        std::vector<double> zeros(std::max(b->nparams[i], 1), 0.0);
-        for (size_t k = 0; k < gops.size(); ++k)
-            LQ_TRY(make_gate_op(&b->ops[i][k], zeros.data(), n, &gops[k]));
+        std::vector<GateOp> gops;
+        std::vector<std::vector<int>> members;
+        LQ_TRY(merge_single_qubit_runs(b->ops[i], n, gops, members));
         std::vector<PlanStep> steps = plan_circuit(gops, n, T);
         for (auto &st : steps)
             if (!st.fused)
@@ -360,7 +518,7 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
                     if (fops.back().type == F_M2 || fops.back().type >= F_BLOCK3)
                         return set_error(LQ_ERR_UNSUPPORTED,
                                          "batched engine: 4x4 gates are not supported");
-                    pg.op_gate[i].push_back(gi);
+                    pg.op_members[i].push_back(members[gi]);
                 }
                 fr.op_end = (int)fops.size();
                 rounds.push_back(fr);
@@ -373,18 +531,22 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
         size_t alt = coef_local.size();
         for (int k = 0; k < pg.nops[i]; ++k) {
             FusedOp &f = fops[pg.op_begin[i] + k];
-            const lq_gate &g = b->ops[i][pg.op_gate[i][k]];
-            int p = -1;
-            for (int a = 0; a < 3; ++a)
-                if (g.param[a] >= 0) {
-                    if (p >= 0 && g.param[a] != p)
-                        return set_error(LQ_ERR_UNSUPPORTED,
-                                         "batched engine: a gate bound to two parameters");
-                    p = g.param[a];
-                }
-            f.param = p;
-            if (p >= 0) {
+            int bound[2] = {-1, -1};
+            for (int gi : pg.op_members[i][k]) {
+                int p;
+                LQ_TRY(gate_param(b->ops[i][gi], &p));
+                if (p < 0 || p == bound[0] || p == bound[1]) continue;
+                if (bound[0] < 0) bound[0] = p;
+                else bound[1] = p;
+            }
+            f.param = bound[0];
+            f.param2 = bound[1];
+            if (bound[0] >= 0) {
                 f.coef_alt = (int)alt;
+                alt += f.type == F_M2 ? 64 : 16;
+            }
+            if (bound[1] >= 0) {
+                f.coef_alt2 = (int)alt;
                 alt += 16;
             }
         }
@@ -394,6 +556,7 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
         pg.h_insts.push_back(in);
     }
     pg.ncoef = coef_off;
+    pg.h_ops = fops;
     // energy windows are shared by the programs (set in lq_batch_create)
     LQ_CUDA_TRY(cudaMalloc(&pg.rounds, sizeof(FusedRound) * std::max<size_t>(rounds.size(), 1)));
     LQ_CUDA_TRY(cudaMalloc(&pg.ops, sizeof(FusedOp) * std::max<size_t>(fops.size(), 1)));
@@ -416,34 +579,33 @@ static int fill_coefficients(lq_batch *b, BProgram &pg, const double *theta, dou
         const double *th = theta + b->param_off[i];
         std::vector<double> tp(th, th + b->nparams[i]);
         double *blk = out + pg.h_insts[i].coef_base;
+        // base coefficients in encode order, then the alt blocks of every
+        // parameter-bound op: (+s, -s) for its first parameter, then its second
         size_t base = 0;
-        size_t alt_end = 0;
-        // base coefficients in encode order, then the alt blocks
         for (int k = 0; k < pg.nops[i]; ++k) {
-            const lq_gate &g = b->ops[i][pg.op_gate[i][k]];
-            GateOp op;
-            LQ_TRY(make_gate_op(&g, tp.data(), n, &op));
-            const int nc = op.type == OP_M2 ? 32 : 8;
-            for (int q = 0; q < nc; ++q) blk[base + q] = (op.type == OP_PERM1 || op.type == OP_SWAP)
-                                                             ? 0.0
-                                                             : op.m[q];
-            base += nc;
-        }
-        alt_end = base;
-        for (int k = 0; k < pg.nops[i]; ++k) {
-            const lq_gate &g = b->ops[i][pg.op_gate[i][k]];
-            int p = -1;
-            for (int a = 0; a < 3; ++a)
-                if (g.param[a] >= 0) p = g.param[a];
-            if (p < 0) continue;
-            for (int sgn = 0; sgn < 2; ++sgn) {
-                tp[p] = th[p] + (sgn == 0 ? shift : -shift);
+            const auto &mem = pg.op_members[i][k];
+            LQ_TRY(op_coefficients(b->ops[i], mem, tp.data(), n, blk + base));
+            bool m2 = false;
+            if (mem.size() == 1) {
                 GateOp op;
-                LQ_TRY(make_gate_op(&g, tp.data(), n, &op));
-                for (int q = 0; q < 8; ++q) blk[alt_end + q] = op.m[q];
-                alt_end += 8;
+                LQ_TRY(make_gate_op(&b->ops[i][mem[0]], tp.data(), n, &op));
+                m2 = op.type == OP_M2;
             }
-            tp[p] = th[p];
+            base += m2 ? 32 : 8;
+        }
+        size_t alt_end = base;
+        for (int k = 0; k < pg.nops[i]; ++k) {
+            const FusedOp &f = pg.h_ops[pg.op_begin[i] + k];
+            const auto &mem = pg.op_members[i][k];
+            for (int p : {f.param, f.param2}) {
+                if (p < 0) continue;
+                for (int sgn = 0; sgn < 2; ++sgn) {
+                    tp[p] = th[p] + (sgn == 0 ? shift : -shift);
+                    LQ_TRY(op_coefficients(b->ops[i], mem, tp.data(), n, blk + alt_end));
+                    alt_end += 8;
+                }
+                tp[p] = th[p];
+            }
         }
     }
     return LQ_OK;
@@ -730,10 +892,27 @@ int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *e
     return LQ_OK;
 }
 
-int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *threads_per_cta) {
+int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits) {
     if (!b) return set_error(LQ_ERR_INVALID_ARG, "null batch");
     if (smem_max_qubits) *smem_max_qubits = kSmemStateMax;
-    if (threads_per_cta) *threads_per_cta = b->chosen >= 0 ? b->progs[b->chosen].T : 0;
+    if (tile_bits) *tile_bits = b->chosen >= 0 ? b->progs[b->chosen].T : 0;
+    return LQ_OK;
+}
+
+int lq_batch_set_tile_bits(lq_batch *b, int tile_bits) {
+    if (!b) return set_error(LQ_ERR_INVALID_ARG, "null batch");
+    int pick = -1;
+    for (size_t pi = 0; pi < b->progs.size(); ++pi)
+        if (b->progs[pi].T == tile_bits) pick = (int)pi;
+    if (tile_bits != 0 && pick < 0)
+        return set_error(LQ_ERR_INVALID_ARG, "tile bits %d not among the planned widths (10-12)",
+                         tile_bits);
+    // the captured graph belongs to the previous choice
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->chosen = pick;  // -1: autotune again on the next lq_batch_gradients call
     return LQ_OK;
 }
 

@@ -3,13 +3,11 @@
 //
 // A pass owns a window W of T <= 12 index bits: the four lowest bits (so every
 // global access is a 256-byte contiguous run) plus a contiguous range
-// [h, h+T-4).  A persistent CTA walks the 2^(n-T) tiles of the state; each
-// tile (2^T amplitudes, 32 KiB of complex128 at T = 11) is staged from HBM
-// into shared memory by one TMA tensor copy (128-byte swizzle) while the CTA
-// computes on the previous tile (two buffers), every gate of the pass is
-// applied, and the tile goes back by an asynchronous TMA store.  HBM traffic
-// per pass is one read and one write of the state, however many gates the
-// pass holds.
+// [h, h+T-4).  One CTA per tile (2^T amplitudes, 32 KiB of complex128 at
+// T = 11): the tile is staged from HBM into shared memory by one TMA tensor
+// copy (128-byte swizzle), every gate of the pass is applied, and the tile
+// goes back by a TMA store.  HBM traffic per pass is one read and one write of
+// the state, however many gates the pass holds.
 //
 // Inside the CTA the gates run in "rounds" (fused_core.cuh): a round picks four
 // tile bits R, each thread gathers the 16 amplitudes that differ only in R
@@ -31,6 +29,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <complex>
 #include <mutex>
 
 #include "fused_plan.h"
@@ -50,8 +49,9 @@ struct TileCoords {
 // (Measured on B200: more resident CTAs per SM beat a persistent,
 // double-buffered CTA here, because the register-resident gate math needs the
 // warps to hide FP64 latency more than it needs load/compute overlap.)
-// EXT selects the variant that also carries 4x4 and block ops (more registers).
-template <bool EXT>
+// MODE selects the op set: 0 = 2x2 / X / diagonal / swap, 1 = also 4x4 ops,
+// 2 = also 8x8 / 16x16 block ops (more registers per mode).
+template <int MODE>
 __global__ void __launch_bounds__(256, 2)
     k_fused_pass(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                  const FusedRound *__restrict__ rounds, int nrounds,
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256, 2)
     const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
     auto coef_of = [&](const FusedOp &op) { return coef + op.coef; };
     for (int r = 0; r < nrounds; ++r) {
-        run_round<EXT>(tile_a, rounds[r], ops, coef_of, tile_base, tc.h, tid);
+        run_round<MODE>(tile_a, rounds[r], ops, coef_of, tile_base, tc.h, tid);
         __syncthreads();
     }
     // Make the generic-proxy writes visible to the TMA engine, then store.
@@ -202,6 +202,199 @@ static void pad_rpos(std::vector<int> &R, int T) {
             if (pass == 0 && conflicts(p)) continue;
             R.push_back(p);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pair folding: (U_x (x) U_y) followed by a two-qubit gate G on bits (x, y)
+// becomes ONE 4x4 op G (U_x (x) U_y).  In a U3 + CNOT layer this replaces two
+// 2x2 ops and a register permutation by one 4x4 op with the same FP64 work
+// and a third of the op overhead.  Runs of single-qubit gates on one bit are
+// merged first.  Host FP64 products; only the fused path folds.
+// ---------------------------------------------------------------------------
+
+// Amplitude map of op g restricted to index bits {bx (hi), by (lo)} (other
+// bits 0, or g touches only these): out[r*4+c] = <r| g |c>, complex.
+static bool op_matrix4(const GateOp &g, int bx, int by, std::complex<double> out[16]) {
+    auto bit_of = [&](int v, int b) -> int { return b == bx ? (v >> 1) & 1 : b == by ? v & 1 : -1; };
+    for (int c = 0; c < 4; ++c) {
+        std::complex<double> col[4] = {0, 0, 0, 0};
+        switch (g.type) {
+        case OP_M1:
+        case OP_PERM1: {
+            bool on = true;
+            for (int k = 0; k < g.nctrl; ++k) {
+                const int v = bit_of(c, g.ctrl[k]);
+                if (v < 0) return false;
+                on = on && v == 1;
+            }
+            const int tv = bit_of(c, g.t);
+            if (tv < 0) return false;
+            if (!on) {
+                col[c] = 1.0;
+                break;
+            }
+            const int tmask = g.t == bx ? 2 : 1;
+            const int c0 = c & ~tmask, c1 = c | tmask;
+            if (g.type == OP_PERM1) {
+                col[c ^ tmask] = 1.0;
+            } else {
+                // column tv of the 2x2 goes to rows (t = 0, t = 1)
+                col[c0] = {g.m[(0 * 2 + tv) * 2], g.m[(0 * 2 + tv) * 2 + 1]};
+                col[c1] = {g.m[(1 * 2 + tv) * 2], g.m[(1 * 2 + tv) * 2 + 1]};
+            }
+            break;
+        }
+        case OP_DIAG: {
+            bool on = true;
+            for (int k = 0; k < g.nfix; ++k) {
+                const int v = bit_of(c, g.fix[k]);
+                if (v < 0) return false;
+                on = on && v == 1;
+            }
+            int pat = 0;
+            for (int k = 0; k < g.npat; ++k) {
+                const int v = bit_of(c, g.pat[k]);
+                if (v < 0) return false;
+                pat |= v << k;
+            }
+            col[c] = on ? std::complex<double>(g.m[2 * pat], g.m[2 * pat + 1]) : 1.0;
+            break;
+        }
+        case OP_SWAP: {
+            if (bit_of(c, g.b0) < 0 || bit_of(c, g.b1) < 0) return false;
+            const int v0 = bit_of(c, g.b0), v1 = bit_of(c, g.b1);
+            int r = 0;
+            r |= (g.b0 == bx ? v1 : v0) << 1;  // bit bx takes the value of its partner
+            r |= (g.b0 == bx ? v0 : v1);
+            col[r] = 1.0;
+            break;
+        }
+        case OP_M2: {
+            // M2 index = (bit b0) << 1 | (bit b1)
+            if (bit_of(c, g.b0) < 0 || bit_of(c, g.b1) < 0) return false;
+            const int ci = (bit_of(c, g.b0) << 1) | bit_of(c, g.b1);
+            for (int ri = 0; ri < 4; ++ri) {
+                const int vb0 = (ri >> 1) & 1, vb1 = ri & 1;
+                const int r = ((g.b0 == bx ? vb0 : vb1) << 1) | (g.b0 == bx ? vb1 : vb0);
+                col[r] = {g.m[(ri * 4 + ci) * 2], g.m[(ri * 4 + ci) * 2 + 1]};
+            }
+            break;
+        }
+        default: return false;
+        }
+        for (int r = 0; r < 4; ++r) out[r * 4 + c] = col[r];
+    }
+    return true;
+}
+
+// 2x2 of an uncontrolled single-qubit op and its bit; false for anything else.
+static bool single_matrix(const GateOp &g, int &bit, std::complex<double> u[4]) {
+    if (g.renorm) return false;
+    if ((g.type == OP_M1 || g.type == OP_PERM1) && g.nctrl == 0) {
+        bit = g.t;
+        if (g.type == OP_M1)
+            for (int k = 0; k < 4; ++k) u[k] = {g.m[2 * k], g.m[2 * k + 1]};
+        else
+            u[0] = 0.0, u[1] = 1.0, u[2] = 1.0, u[3] = 0.0;
+        return true;
+    }
+    if (g.type == OP_DIAG && g.nfix == 0 && g.npat == 1) {
+        bit = g.pat[0];
+        u[0] = {g.m[0], g.m[1]}, u[1] = 0.0, u[2] = 0.0, u[3] = {g.m[2], g.m[3]};
+        return true;
+    }
+    return false;
+}
+
+static void fold_pairs(std::vector<GateOp> &gops, std::vector<int> &orig, int T) {
+    struct Entry {
+        GateOp op;
+        int orig;
+        bool dead;
+        bool single;
+        int bit;
+        std::complex<double> u[4];
+    };
+    std::vector<Entry> out;
+    std::vector<int> open(64, -1);  // per bit: the pending single-qubit entry
+    for (size_t k = 0; k < gops.size(); ++k) {
+        const GateOp &g = gops[k];
+        Entry e{g, (int)k, false, false, -1, {}};
+        int bit;
+        std::complex<double> u[4];
+        if (single_matrix(g, bit, u)) {
+            if (open[bit] >= 0) {  // extend the run: U_run <- u . U_run
+                Entry &r = out[open[bit]];
+                std::complex<double> p[4] = {u[0] * r.u[0] + u[1] * r.u[2],
+                                             u[0] * r.u[1] + u[1] * r.u[3],
+                                             u[2] * r.u[0] + u[3] * r.u[2],
+                                             u[2] * r.u[1] + u[3] * r.u[3]};
+                const bool diag = r.op.type == OP_DIAG && g.type == OP_DIAG;
+                GateOp m{};
+                if (diag) {
+                    m.type = OP_DIAG;
+                    m.npat = 1;
+                    m.pat[0] = bit;
+                    m.m[0] = p[0].real(), m.m[1] = p[0].imag();
+                    m.m[2] = p[3].real(), m.m[3] = p[3].imag();
+                } else {
+                    m.type = OP_M1;
+                    m.t = bit;
+                    for (int q = 0; q < 4; ++q) m.m[2 * q] = p[q].real(), m.m[2 * q + 1] = p[q].imag();
+                }
+                r.op = m;
+                r.orig = -1;
+                for (int q = 0; q < 4; ++q) r.u[q] = p[q];
+                continue;
+            }
+            e.single = true;
+            e.bit = bit;
+            for (int q = 0; q < 4; ++q) e.u[q] = u[q];
+            out.push_back(e);
+            open[bit] = (int)out.size() - 1;
+            continue;
+        }
+        const uint64_t bits = op_bits(g);
+        if (!g.renorm && popc(bits) == 2) {
+            const int bx = 63 - __builtin_clzll(bits), by = __builtin_ctzll(bits);
+            std::complex<double> G[16];
+            // both bits must fit one window [0,4) U [h, h+T-4) (else a standalone sweep)
+            const bool fits = by < 4 || bx - by < T - 4;
+            if (fits && open[bx] >= 0 && open[by] >= 0 && op_matrix4(g, bx, by, G)) {
+                Entry &ex = out[open[bx]], &ey = out[open[by]];
+                // M = G . (U_x (x) U_y), index (bit bx) << 1 | (bit by)
+                std::complex<double> K[16], M[16];
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c)
+                        K[r * 4 + c] = ex.u[(r >> 1) * 2 + (c >> 1)] * ey.u[(r & 1) * 2 + (c & 1)];
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) {
+                        std::complex<double> s = 0.0;
+                        for (int q = 0; q < 4; ++q) s += G[r * 4 + q] * K[q * 4 + c];
+                        M[r * 4 + c] = s;
+                    }
+                ex.dead = ey.dead = true;
+                GateOp m{};
+                m.type = OP_M2;
+                m.b0 = bx;
+                m.b1 = by;
+                for (int q = 0; q < 16; ++q) m.m[2 * q] = M[q].real(), m.m[2 * q + 1] = M[q].imag();
+                out.push_back(Entry{m, -1, false, false, -1, {}});
+                open[bx] = open[by] = -1;
+                continue;
+            }
+        }
+        for (int b = 0; b < 64; ++b)
+            if ((bits >> b) & 1) open[b] = -1;
+        out.push_back(e);
+    }
+    gops.clear();
+    orig.clear();
+    for (auto &e : out) {
+        if (e.dead) continue;
+        gops.push_back(e.op);
+        orig.push_back(e.orig);
     }
 }
 
@@ -329,8 +522,8 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
     FusedOp f{};
     f.coef = (int)coef.size();
     f.pb0 = f.pb1 = -1;
-    f.param = -1;
-    f.coef_alt = -1;
+    f.param = f.param2 = -1;
+    f.coef_alt = f.coef_alt2 = -1;
     switch (g.type) {
     case OP_M1:
     case OP_PERM1: {
@@ -366,12 +559,26 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
         f.k1 = reg(g.b1);
         coef.insert(coef.end(), 8, 0.0);
         break;
-    case OP_M2:
+    case OP_M2: {
+        // register bits ordered k0 < k1 (the kernel unrolls only those pairs):
+        // swapping the bits swaps the two bits of the 4x4 row / column index
         f.type = F_M2;
-        f.k0 = reg(g.b0);
-        f.k1 = reg(g.b1);
-        coef.insert(coef.end(), g.m, g.m + 32);
+        int k0 = reg(g.b0), k1 = reg(g.b1);
+        if (k0 < k1) {
+            coef.insert(coef.end(), g.m, g.m + 32);
+        } else {
+            std::swap(k0, k1);
+            const int sw[4] = {0, 2, 1, 3};
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) {
+                    coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2]);
+                    coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2 + 1]);
+                }
+        }
+        f.k0 = k0;
+        f.k1 = k1;
         break;
+    }
     }
     fops.push_back(f);
 }
@@ -379,14 +586,13 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
 struct PassLaunch {
     int h;
     int round_begin, nrounds;
-    bool extended;  // holds 4x4 / block ops: needs the extended kernel variant
+    int mode;  // kernel op set the pass needs (k_fused_pass MODE)
 };
 
 static size_t fused_smem(int T) { return (16u << T) + 2048; }
 
-static int fused_grid(int T, int ntiles, bool extended) {
+static int fused_grid(int T, int ntiles) {
     (void)T;
-    (void)extended;
     return ntiles;
 }
 
@@ -394,31 +600,36 @@ static int set_smem_attrs() {
     static bool done = false;
     if (done) return LQ_OK;
     const int mx = (int)fused_smem(kMaxT);
-    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<false>,
+    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<0>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<true>,
+    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<1>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    LQ_CUDA_TRY(cudaFuncSetAttribute(k_fused_pass<2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     done = true;
     return LQ_OK;
 }
 
 static int launch_pass(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
-                       const FusedOp *d_ops, const double *d_coef, bool extended) {
+                       const FusedOp *d_ops, const double *d_coef, int mode) {
     const int n = s->n;
     const int m = T - 4;
     CUtensorMap map;
     LQ_TRY(make_tile_map(&map, s->d, n, h, m));
     const int ntiles = 1 << (n - T);
     TileCoords tc{h, h + m, ntiles};
-    const int grid = fused_grid(T, ntiles, extended);
+    const int grid = fused_grid(T, ntiles);
     const size_t smem = fused_smem(T);
     prof_begin(s->stream, kProfFused);
-    if (extended)
-        k_fused_pass<true><<<grid, 1 << (T - 4), smem, s->stream>>>(map, T, tc, d_rounds, nrounds,
-                                                                    d_ops, d_coef, s->d_flag);
+    if (mode == 2)
+        k_fused_pass<2><<<grid, 1 << (T - 4), smem, s->stream>>>(map, T, tc, d_rounds, nrounds,
+                                                                 d_ops, d_coef, s->d_flag);
+    else if (mode == 1)
+        k_fused_pass<1><<<grid, 1 << (T - 4), smem, s->stream>>>(map, T, tc, d_rounds, nrounds,
+                                                                 d_ops, d_coef, s->d_flag);
     else
-        k_fused_pass<false><<<grid, 1 << (T - 4), smem, s->stream>>>(
-            map, T, tc, d_rounds, nrounds, d_ops, d_coef, s->d_flag);
+        k_fused_pass<0><<<grid, 1 << (T - 4), smem, s->stream>>>(map, T, tc, d_rounds, nrounds,
+                                                                 d_ops, d_coef, s->d_flag);
     prof_end(s->stream, kProfFused);
     LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
@@ -430,14 +641,15 @@ static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<G
                          std::vector<double> &coef, std::vector<PassLaunch> &launches) {
     for (auto &st : steps) {
         if (!st.fused) continue;
-        PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), false};
+        PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), 0};
         for (auto &rd : st.pass.rounds) {
             FusedRound fr{};
             fill_round(fr, rd.rpos, T, st.pass.h);
             fr.op_begin = (int)fops.size();
             for (int k : rd.ops) {
                 encode_op(gops[st.pass.gates[k]], st.pass.h, T - 4, rd.rpos, fops, coef);
-                if (fops.back().type == F_M2) pl.extended = true;
+                if (fops.back().type == F_M2) pl.mode = std::max(pl.mode, 1);
+                if (fops.back().type >= F_BLOCK3) pl.mode = 2;
             }
             fr.op_end = (int)fops.size();
             rounds.push_back(fr);
@@ -465,6 +677,8 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
         return LQ_OK;
     }
     const int T = std::min(fusion_width(), n);
+    std::vector<int> orig;
+    fold_pairs(gops, orig, T);
     std::vector<PlanStep> steps = plan_circuit(gops, n, T);
     std::vector<FusedRound> rounds;
     std::vector<FusedOp> fops;
@@ -496,7 +710,7 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
         }
         const PassLaunch &pl = launches[li++];
         LQ_TRY(launch_pass(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef,
-                           pl.extended));
+                           pl.mode));
         s->last_launches += 1;
         s->last_passes += 1;
     }
@@ -538,7 +752,7 @@ int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m) {
     FusedOp fo{};
     fo.type = k == 3 ? F_BLOCK3 : F_BLOCK4;
     fo.pb0 = fo.pb1 = -1;
-    fo.param = fo.coef_alt = -1;
+    fo.param = fo.coef_alt = fo.param2 = fo.coef_alt2 = -1;
     fo.coef = 0;
     const size_t cb = sizeof(double) * 2 * (1 << k) * (1 << k);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -552,7 +766,7 @@ int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m) {
     LQ_CUDA_TRY(cudaMemcpy(d_ops, &fo, sizeof(FusedOp), cudaMemcpyHostToDevice));
     LQ_CUDA_TRY(cudaMemcpy(d_coef, m, cb, cudaMemcpyHostToDevice));
     LQ_TRY(set_smem_attrs());
-    return launch_pass(s, T, h, d_rounds, 1, d_ops, d_coef, true);
+    return launch_pass(s, T, h, d_rounds, 1, d_ops, d_coef, 2);
 }
 
 }  // namespace lq
@@ -602,7 +816,7 @@ int lq_apply_block(lq_state *s, int k, const int *qubits, const double *m) {
 
 static int plan_for(int num_qubits, const lq_gate *ops, int nops, const double *theta,
                     int ntheta, std::vector<GateOp> &gops, std::vector<PlanStep> &steps,
-                    int &T) {
+                    int &T, std::vector<int> &orig) {
     if (nops < 0 || (nops > 0 && !ops)) return set_error(LQ_ERR_INVALID_ARG, "bad op list");
     if (num_qubits < 5 || num_qubits > 36)
         return set_error(LQ_ERR_UNSUPPORTED, "fused planning needs 5..36 qubits");
@@ -617,6 +831,7 @@ static int plan_for(int num_qubits, const lq_gate *ops, int nops, const double *
         LQ_TRY(make_gate_op(&g, theta ? theta : zero_theta, num_qubits, &gops[i]));
     }
     T = std::min(fusion_width(), num_qubits);
+    fold_pairs(gops, orig, T);
     steps = plan_circuit(gops, num_qubits, T);
     return LQ_OK;
 }
@@ -625,8 +840,9 @@ int lq_plan_circuit(int num_qubits, const lq_gate *ops, int nops, int *passes, i
                     int *standalone) {
     std::vector<GateOp> gops;
     std::vector<PlanStep> steps;
+    std::vector<int> orig;
     int T;
-    LQ_TRY(plan_for(num_qubits, ops, nops, nullptr, 0, gops, steps, T));
+    LQ_TRY(plan_for(num_qubits, ops, nops, nullptr, 0, gops, steps, T, orig));
     int p = 0, r = 0, s1 = 0;
     for (auto &st : steps) {
         if (st.fused) {
@@ -649,8 +865,9 @@ int lq_plan_dump(int num_qubits, const lq_gate *ops, int nops, const double *the
     // nrounds x FusedRound, nops x FusedOp, ncoef x double.
     std::vector<GateOp> gops;
     std::vector<PlanStep> steps;
+    std::vector<int> orig;
     int T;
-    LQ_TRY(plan_for(num_qubits, ops, nops, theta, ntheta, gops, steps, T));
+    LQ_TRY(plan_for(num_qubits, ops, nops, theta, ntheta, gops, steps, T, orig));
     std::vector<FusedRound> rounds;
     std::vector<FusedOp> fops;
     std::vector<double> coef;
@@ -660,7 +877,8 @@ int lq_plan_dump(int num_qubits, const lq_gate *ops, int nops, const double *the
     size_t li = 0;
     for (auto &st : steps) {
         if (!st.fused) {
-            st_rec.insert(st_rec.end(), {0, st.gate, 0, 0, 0});
+            // standalone steps name the caller's gate (they are never folded)
+            st_rec.insert(st_rec.end(), {0, orig[st.gate], 0, 0, 0});
         } else {
             const PassLaunch &pl = launches[li++];
             st_rec.insert(st_rec.end(), {1, -1, pl.h, pl.round_begin, pl.nrounds});

@@ -33,9 +33,12 @@ struct FusedOp {
     int32_t pb0, pb1;  // F_DIAG pattern bit positions (global)
     int32_t npat;
     int32_t coef;      // offset of the coefficients in the coefficient array (doubles)
-    int32_t param;     // batched engine: parameter the op's angle is bound to (-1: none)
-    int32_t coef_alt;  // batched engine: offset of the (+shift, -shift) coefficient pair
+    int32_t param;      // batched engine: parameter the op's angle is bound to (-1: none)
+    int32_t coef_alt;   // batched engine: offset of the (+shift, -shift) coefficient pair
+    int32_t param2;     // batched engine: second bound parameter of a merged op (-1: none)
+    int32_t coef_alt2;  // batched engine: its (+shift, -shift) coefficient pair
 };
+static_assert(sizeof(FusedOp) == 64, "FusedOp layout is mirrored by the plan-dump reader");
 
 struct FusedRound {
     int32_t eoff[16];  // swizzled byte offset of register element e relative to the thread base
@@ -173,7 +176,9 @@ __device__ __forceinline__ void reg_diag(double2 (&a)[16], const FusedOp &op,
 
 // Apply one op.  c8 holds the op's first eight coefficients (prefetched by the
 // caller); cfull points at all of them (4x4 and block ops read more).
-template <bool EXT>
+// MODE 0: 2x2, X, diagonal and swap ops; 1: also 4x4 ops; 2: also 8x8 / 16x16
+// block ops.
+template <int MODE>
 __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &op,
                                                const double (&c8)[8],
                                                const double *__restrict__ cfull, uint64_t gbase,
@@ -234,27 +239,21 @@ __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &
         break;
     }
     default:
-        if constexpr (EXT) {
+        if constexpr (MODE >= 1) {
             if (op.type == F_M2) {
+                // the encoder orders the register bits k0 < k1
                 const int key = op.k0 * 4 + op.k1;
                 switch (key) {
                 case 1: reg_m2<0, 1>(a, cfull); break;
                 case 2: reg_m2<0, 2>(a, cfull); break;
                 case 3: reg_m2<0, 3>(a, cfull); break;
-                case 4: reg_m2<1, 0>(a, cfull); break;
                 case 6: reg_m2<1, 2>(a, cfull); break;
                 case 7: reg_m2<1, 3>(a, cfull); break;
-                case 8: reg_m2<2, 0>(a, cfull); break;
-                case 9: reg_m2<2, 1>(a, cfull); break;
-                case 11: reg_m2<2, 3>(a, cfull); break;
-                case 12: reg_m2<3, 0>(a, cfull); break;
-                case 13: reg_m2<3, 1>(a, cfull); break;
-                default: reg_m2<3, 2>(a, cfull); break;
+                default: reg_m2<2, 3>(a, cfull); break;
                 }
-            } else if (op.type == F_BLOCK3) {
-                reg_block<3>(a, cfull);
-            } else {
-                reg_block<4>(a, cfull);
+            } else if constexpr (MODE >= 2) {
+                if (op.type == F_BLOCK3) reg_block<3>(a, cfull);
+                else reg_block<4>(a, cfull);
             }
         }
         break;
@@ -264,7 +263,7 @@ __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &
 // One round on a tile in shared memory: gather 16 registers per thread, run
 // the round's ops (op descriptors and their first coefficients prefetched one
 // op ahead), scatter back.  coef_of(op) returns the op's coefficient pointer.
-template <bool EXT, class CoefOf>
+template <int MODE, class CoefOf>
 __device__ __forceinline__ void run_round(uint32_t tile_a, const FusedRound &rd,
                                           const FusedOp *__restrict__ ops, CoefOf coef_of,
                                           uint64_t tile_base, int h, int tid) {
@@ -298,7 +297,7 @@ __device__ __forceinline__ void run_round(uint32_t tile_a, const FusedRound &rd,
 #pragma unroll
                 for (int q = 0; q < 8; ++q) nc[q] = ncp[q];
             }
-            apply_fused_op<EXT>(a, op, cc, cp, gbase, rd.gpos);
+            apply_fused_op<MODE>(a, op, cc, cp, gbase, rd.gpos);
         }
     }
 #pragma unroll

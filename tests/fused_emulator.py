@@ -18,7 +18,8 @@ ROUND_DT = np.dtype([("eoff", np.int32, 16), ("gpos", np.uint64, 4), ("lane", np
 OP_DT = np.dtype([("type", np.int32), ("k0", np.int32), ("k1", np.int32), ("cm", np.int32),
                   ("gmask", np.uint64), ("fixmask", np.uint64), ("pb0", np.int32),
                   ("pb1", np.int32), ("npat", np.int32), ("coef", np.int32),
-                  ("param", np.int32), ("coef_alt", np.int32)], align=True)
+                  ("param", np.int32), ("coef_alt", np.int32), ("param2", np.int32),
+                  ("coef_alt2", np.int32)], align=True)
 
 F_M1, F_M1C, F_X, F_XC, F_DIAG, F_SWAP, F_M2, F_BLOCK3, F_BLOCK4 = range(9)
 

@@ -76,3 +76,32 @@ def test_batch_mixed_sizes_and_new_theta():
         terms = workloads.heisenberg_terms(n, r["jx"], r["jy"], r["jz"], r["h"])
         _, g_plain = plain_gradient(n, gates, r["theta"] + 0.1, terms)
         assert np.abs(gs[i] - g_plain).max() < 1e-10
+
+
+@pytest.mark.parametrize("tile_bits", [10, 11, 12])
+def test_batch_every_tile_width_matches_plain(tile_bits):
+    """Each fusion width the autotuner may pick gives the plain path's gradients
+    (at widths below 12 only part of the CTA's threads own amplitudes)."""
+    recs = workloads.heisenberg_instances(3, seed=21, n_lo=13, n_hi=15)
+    b = heisenberg_batch(recs)
+    call("lq_batch_set_tile_bits", b._h, tile_bits)
+    theta = np.concatenate([r["theta"] for r in recs])
+    e, g = b.gradients(theta)
+    assert b.tuning()["tile_bits"] == tile_bits
+    gs = b.split(g)
+    for i, r in enumerate(recs):
+        n = r["n"]
+        gates = workloads.basic_entangling_template(n, 4)
+        terms = workloads.heisenberg_terms(n, r["jx"], r["jy"], r["jz"], r["h"])
+        e_plain, g_plain = plain_gradient(n, gates, r["theta"], terms)
+        assert abs(e[i] - e_plain) < 1e-12 * max(1, abs(e_plain))
+        assert np.abs(gs[i] - g_plain).max() < 1e-10
+
+
+def test_batch_set_tile_bits_rejects_unknown_width():
+    from logosq_b200 import LogosQError
+    b = heisenberg_batch(workloads.heisenberg_instances(1, seed=2, n_lo=13, n_hi=13))
+    with pytest.raises(LogosQError) as e:
+        call("lq_batch_set_tile_bits", b._h, 9)
+    assert e.value.code == abi.LQ_ERR_INVALID_ARG
+    call("lq_batch_set_tile_bits", b._h, 0)  # back to autotuning
