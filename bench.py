@@ -624,8 +624,8 @@ def main():
     fused_launch_ms = fused_ms.value / max(fused_n.value, 1)
     achieved = 2 * S / (fused_launch_ms / 1e3) / 1e9 if fused_n.value else None
     # ncu (profiles/k_fused_pass_brickwork26q.md): dram read + write per launch at 26
-    # qubits = 2.096e9 B (0.976 x 2S); a launch sweeps the whole state, so scale by 2^(n-26).
-    traffic = 2.096e9 * 2.0 ** (n - 26)
+    # qubits = 2.11e9 B (0.98 x 2S); a launch sweeps the whole state, so scale by 2^(n-26).
+    traffic = 2.11e9 * 2.0 ** (n - 26)
     n_u3 = int(np.sum(gates["kind"] == abi.U3))
     fp64_flops_step = 14.0 * n_u3 * (1 << n)  # 2x2 complex matrix: 14 flops per amplitude
     roofline = {"kernel": "k_fused_pass (TMA-staged 2^T-amplitude tiles)", "bound": "hbm",
