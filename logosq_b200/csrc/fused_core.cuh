@@ -105,28 +105,47 @@ __device__ __forceinline__ void reg_swap(double2 (&a)[16]) {
     }
 }
 
+// 4x4 on register bits (K0, K1): four groups of four amplitudes.  The groups
+// go two at a time so that each coefficient (one 16-byte load) serves two
+// groups, with 16 accumulators live beside the 16 registers.
 template <int K0, int K1>
 __device__ __forceinline__ void reg_m2(double2 (&a)[16], const double *__restrict__ c) {
+    const double2 *__restrict__ cm = reinterpret_cast<const double2 *>(c);
+    int grp[4], ng = 0;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
-        const int idx[4] = {e, e | (1 << K1), e | (1 << K0), e | (1 << K0) | (1 << K1)};
-        double2 in[4], out[4];
+    for (int e = 0; e < 16; ++e)
+        if (!(e & (1 << K0)) && !(e & (1 << K1))) grp[ng++] = e;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) in[r] = a[idx[r]];
+    for (int gp = 0; gp < 2; ++gp) {
+        int idx[2][4];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int e = grp[2 * gp + s];
+            idx[s][0] = e;
+            idx[s][1] = e | (1 << K1);
+            idx[s][2] = e | (1 << K0);
+            idx[s][3] = e | (1 << K0) | (1 << K1);
+        }
+        double2 out[2][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            double ore = 0.0, oim = 0.0;
+            double o0r = 0.0, o0i = 0.0, o1r = 0.0, o1i = 0.0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const double mr = c[(r * 4 + q) * 2], mi = c[(r * 4 + q) * 2 + 1];
-                ore = fma(-mi, in[q].y, fma(mr, in[q].x, ore));
-                oim = fma(mi, in[q].x, fma(mr, in[q].y, oim));
+                const double2 m = cm[r * 4 + q];
+                const double2 x0 = a[idx[0][q]], x1 = a[idx[1][q]];
+                o0r = fma(-m.y, x0.y, fma(m.x, x0.x, o0r));
+                o0i = fma(m.y, x0.x, fma(m.x, x0.y, o0i));
+                o1r = fma(-m.y, x1.y, fma(m.x, x1.x, o1r));
+                o1i = fma(m.y, x1.x, fma(m.x, x1.y, o1i));
             }
-            out[r] = make_double2(ore, oim);
+            out[0][r] = make_double2(o0r, o0i);
+            out[1][r] = make_double2(o1r, o1i);
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) a[idx[r]] = out[r];
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[idx[s][r]] = out[s][r];
     }
 }
 

@@ -4,19 +4,22 @@
 //     X W ~= Xh Wh + Xh Wl + Xl Wh,   Xh = tf32(X), Xl = tf32(X - Xh).
 //
 // A pass owns a window of T = 12 index bits ([0,4) U [h, h+8), as the FP64
-// fused passes).  Each CTA stages one 2^12-amplitude complex64 tile (32 KiB) by
-// TMA (128-byte swizzle) and applies the pass's blocks in order.  For a block
-// on tile bits k0..k4 the tile is a 128 x 32 complex matrix X (rows: the other
-// seven tile bits; columns: the block index).  Viewed as reals interleaved
-// (re, im) it is X' (128 x 64) and the block is Y' = X' W' with the real
-// 64 x 64 matrix W' = [[Re U^T, Im U^T], [-Im U^T, Re U^T]] interleaved the
-// same way.  The 128 threads gather X' into two K-major 128-byte-swizzled
-// operand buffers (hi and lo TF32 parts), one elected thread issues 3 x 8
-// tcgen05.mma (K = 8 each) into a 128-lane x 64-column FP32 accumulator in
-// TMEM, commits to an mbarrier, and each warp reads its 32 lanes back with
-// tcgen05.ld and scatters the rows into the tile.  The tile is written back
-// by one TMA store.  W' hi/lo are prepared on the host (FP64 -> TF32 splits)
-// already in the swizzled byte order of the B operand.
+// fused passes) and applies its 5-qubit blocks to every 2^12-amplitude
+// complex64 tile (32 KiB, TMA with 128-byte swizzle).  For a block on tile bits
+// k0..k4 the tile is a 128 x 32 complex matrix X (rows: the other seven tile
+// bits; columns: the block index).  Viewed as reals interleaved (re, im) it is
+// X' (128 x 64) and the block is Y' = X' W' with the real 64 x 64 matrix
+// W' = [[Re U^T, Im U^T], [-Im U^T, Re U^T]] interleaved the same way.
+//
+// Thread m owns GEMM row m, which is also tensor-memory lane m: it splits its
+// row into TF32 hi / lo parts and writes them to tensor memory (tcgen05.st);
+// one elected thread issues 3 x 8 tcgen05.mma (K = 8 each) with A read from
+// tensor memory and B (W' hi / lo, prepared on the host in the swizzled K-major
+// byte order and brought in by one bulk copy) from shared memory, into a
+// 128-lane x 64-column FP32 accumulator; each thread reads its row back with
+// tcgen05.ld and scatters it into the tile.  CTAs are persistent (two per SM:
+// 97 KiB of shared memory and 256 tensor-memory columns each), prefetch their
+// next tile into a second buffer and store finished tiles asynchronously.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -29,13 +32,15 @@
 
 namespace lq {
 
-constexpr int kTcT = 12;                // tile bits
-constexpr int kTcRows = 1 << (kTcT - 5);  // 128 GEMM rows per tile
-constexpr int kTcThreads = 128;
-constexpr uint32_t kTileBytes = 8u << kTcT;          // 32 KiB complex64 tile
-constexpr uint32_t kABytes = kTcRows * 64 * 4;       // 32 KiB per A part (hi / lo)
-constexpr uint32_t kBBytes = 64 * 64 * 4;            // 16 KiB per B part (hi / lo)
-constexpr uint32_t kTcSmem = kTileBytes + 2 * kABytes + 2 * kBBytes + 1024 + 64;
+constexpr int kTcT = 12;                  // tile bits
+constexpr int kTcThreads = 128;           // thread m owns GEMM row m = TMEM lane m
+constexpr uint32_t kTileBytes = 8u << kTcT;  // 32 KiB complex64 tile
+constexpr uint32_t kBBytes = 64 * 64 * 4;    // 16 KiB per B part (hi / lo)
+// shared memory: two tile buffers, B hi + lo, barriers
+constexpr uint32_t kTcSmem = 2 * kTileBytes + 2 * kBBytes + 1024 + 128;
+// tensor memory columns: D (FP32 accumulator) [0,64), A hi [64,128), A lo [128,192)
+constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kColD = 0, kColAh = 64, kColAl = 128;
 
 struct TcBlock {
     int32_t k[5];     // tile-local bit of block bit j (block index bit j)
@@ -43,6 +48,7 @@ struct TcBlock {
     uint32_t row_bits[7];  // tile-local positions of the 7 row bits
     uint32_t pad2;
     uint64_t b_offset;  // offset (bytes) of this block's 32 KiB B image (hi then lo)
+    uint32_t col_bits[32];  // tile-local index bits of block column c (its 5 bits placed)
 };
 
 struct TcPass {
@@ -60,13 +66,6 @@ __device__ __forceinline__ uint32_t tc_smem_u32(const void *p) {
 __device__ __forceinline__ uint32_t tile_off(uint32_t l) {
     const uint32_t row = l >> 4, chunk = (l & 15) >> 1;
     return row * 128 + ((chunk ^ (row & 7)) << 4) + ((l & 1) << 3);
-}
-
-// Byte offset of K-major operand element (row m, float k), rows of 128 B per
-// K-atom of 32 floats, 128-byte swizzle, atoms of `rows` rows.
-__device__ __forceinline__ uint32_t kmajor_off(uint32_t m, uint32_t k, uint32_t rows) {
-    const uint32_t atom = k >> 5, kb = (k & 31) * 4;
-    return atom * rows * 128 + m * 128 + (((kb >> 4) ^ (m & 7)) << 4) + (kb & 15);
 }
 
 __device__ __forceinline__ float to_tf32(float x) {
@@ -107,186 +106,238 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) |
                             ((128u >> 4) << 24);
 
-__global__ void __launch_bounds__(kTcThreads, 1)
-    k_tc_pass(const __grid_constant__ CUtensorMap tmap, int32_t h, int32_t hm,
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, "
+        "%10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+        "%10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Persistent CTAs (two per SM), each walking tiles t = blockIdx.x, +gridDim.x.
+// Per tile: TMA load (prefetched one tile ahead into the other buffer), then per
+// 5-qubit block: B image (one bulk copy), A split into TF32 hi / lo written to
+// tensor memory by the owning threads (row m = TMEM lane m), 3 x 8 tcgen05.mma
+// with A from tensor memory, tcgen05.ld of the 128 x 64 FP32 result and scatter
+// into the tile; finally an asynchronous TMA store, waited for only before its
+// buffer is reloaded.
+__global__ void __launch_bounds__(kTcThreads, 2)
+    k_tc_pass(const __grid_constant__ CUtensorMap tmap, int32_t h, int32_t ntiles,
               const TcBlock *__restrict__ blocks, int nblocks,
               const unsigned char *__restrict__ bimg, unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char *tile = base;
-    unsigned char *a_hi = tile + kTileBytes;
-    unsigned char *a_lo = a_hi + kABytes;
-    unsigned char *b_hi = a_lo + kABytes;
+    unsigned char *tiles = base;                       // 2 x 32 KiB
+    unsigned char *b_hi = tiles + 2 * kTileBytes;      // 16 KiB, then b_lo
     unsigned char *b_lo = b_hi + kBBytes;
-    uint64_t *bars = (uint64_t *)(b_lo + kBBytes);  // [0] TMA load, [1] MMA done
-    uint32_t *tmem_slot = (uint32_t *)(bars + 2);
-    const uint32_t tile_a = tc_smem_u32(tile);
-    const uint32_t bar_load = tc_smem_u32(&bars[0]);
-    const uint32_t bar_mma = tc_smem_u32(&bars[1]);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int32_t bid = blockIdx.x;
-    const int32_t c1 = bid & ((1 << (h - 4)) - 1);
-    const int32_t c3 = bid >> (h - 4);
+    uint64_t *bars = (uint64_t *)(b_lo + kBBytes);     // [0],[1] tile loads, [2] B, [3] MMA
+    uint32_t *tmem_slot = (uint32_t *)(bars + 4);
+    int *s_abort = (int *)(tmem_slot + 1);
+    const uint32_t bar_load0 = tc_smem_u32(&bars[0]);
+    const uint32_t bar_b = tc_smem_u32(&bars[2]);
+    const uint32_t bar_mma = tc_smem_u32(&bars[3]);
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int32_t zero = 0;
-    bool ok = true;
 
     if (warp == 0) {
-        // 64 TMEM columns for the 128 x 64 FP32 accumulator
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          tc_smem_u32(tmem_slot)),
-                     "r"(64)
+                     "r"(kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_load), "r"(1) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_mma), "r"(1) : "memory");
+        for (int i = 0; i < 4; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(&bars[i])),
+                         "r"(1)
+                         : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *s_abort = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 
-    if (tid == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_load),
+    auto issue_load = [&](int t, int buf) {
+        const int32_t c1 = t & ((1 << (h - 4)) - 1), c3 = t >> (h - 4);
+        const uint32_t bar = bar_load0 + 8u * buf;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                      "r"(kTileBytes)
                      : "memory");
         asm volatile(
             "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(tile_a),
-            "l"((uint64_t)&tmap), "r"(zero), "r"(c1), "r"(zero), "r"(c3), "r"(bar_load)
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(tc_smem_u32(tiles + buf * kTileBytes)),
+            "l"((uint64_t)&tmap), "r"(zero), "r"(c1), "r"(zero), "r"(c3), "r"(bar)
             : "memory");
-    }
-    if (!tc_wait(bar_load, 0)) ok = false;
+    };
 
-    uint32_t mma_phase = 0;
-    for (int bi = 0; bi < nblocks && ok; ++bi) {
-        const TcBlock blk = blocks[bi];
-        // B operand (hi, lo): prepared swizzled image, plain 16-byte copies
-        {
-            const uint4 *src = (const uint4 *)(bimg + blk.b_offset);
-            uint4 *dst = (uint4 *)b_hi;  // b_hi and b_lo are contiguous
-            for (int i = tid; i < (int)(2 * kBBytes / 16); i += kTcThreads) dst[i] = src[i];
+    uint32_t load_phase[2] = {0u, 0u}, b_phase = 0u, mma_phase = 0u;
+    bool load_pending[2] = {false, false};  // thread 0: a tile load not yet waited for
+    bool mma_pending = false;
+    int buf = 0;
+    if (tid == 0 && (int)blockIdx.x < ntiles) {
+        issue_load(blockIdx.x, 0);
+        load_pending[0] = true;
+    }
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (!tc_wait(bar_load0 + 8u * buf, load_phase[buf])) atomicExch(s_abort, 1);
+        load_phase[buf] ^= 1u;
+        if (tid == 0) load_pending[buf] = false;
+        __syncthreads();
+        if (*s_abort) break;
+        const int tn = t + gridDim.x;
+        if (tid == 0 && tn < ntiles) {
+            // the other buffer's store (previous tile) must have left shared memory
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            issue_load(tn, buf ^ 1);
+            load_pending[buf ^ 1] = true;
         }
-        // A operand: row m = tid, the 32 complex entries of the block
-        {
-            const uint32_t m = tid;
+        unsigned char *tile = tiles + buf * kTileBytes;
+        const uint32_t tile_a = tc_smem_u32(tile);
+        for (int bi = 0; bi < nblocks; ++bi) {
+            const TcBlock &blk = blocks[bi];
+            if (tid == 0) {  // B hi + lo: one 32 KiB bulk copy (prepared swizzled image)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b),
+                             "r"(2 * kBBytes)
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+                    " [%0], [%1], %2, [%3];" ::"r"(tc_smem_u32(b_hi)),
+                    "l"((uint64_t)(bimg + blk.b_offset)), "r"(2 * kBBytes), "r"(bar_b)
+                    : "memory");
+            }
+            // A row m = tid: the block's 32 complex entries, split hi / lo into TMEM
             uint32_t lbase = 0;
 #pragma unroll
-            for (int j = 0; j < 7; ++j) lbase |= ((m >> j) & 1u) << blk.row_bits[j];
-#pragma unroll 4
-            for (uint32_t c = 0; c < 32; ++c) {
-                uint32_t l = lbase;
-#pragma unroll
-                for (int j = 0; j < 5; ++j) l |= ((c >> j) & 1u) << blk.k[j];
-                const float2 v = *(const float2 *)(tile + tile_off(l));
-                const float rh = to_tf32(v.x), ih = to_tf32(v.y);
-                const float rl = to_tf32(v.x - rh), il = to_tf32(v.y - ih);
-                const uint32_t o0 = kmajor_off(m, 2 * c, kTcRows);
-                const uint32_t o1 = kmajor_off(m, 2 * c + 1, kTcRows);
-                *(float *)(a_hi + o0) = rh;
-                *(float *)(a_hi + o1) = ih;
-                *(float *)(a_lo + o0) = rl;
-                *(float *)(a_lo + o1) = il;
-            }
-        }
-        // generic-proxy smem writes -> visible to the tensor-core (async) proxy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (tid == 0) {
-            const uint32_t ah = tc_smem_u32(a_hi), al = tc_smem_u32(a_lo);
-            const uint32_t bh = tc_smem_u32(b_hi), bl = tc_smem_u32(b_lo);
-            const uint32_t pa[3] = {ah, ah, al}, pb[3] = {bh, bl, bh};
-#pragma unroll
-            for (int prod = 0; prod < 3; ++prod) {
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {
-                    // K step kk: 8 TF32 = 32 bytes; atom = kk / 4
-                    const uint32_t aoff = (kk >> 2) * (kTcRows * 128) + (kk & 3) * 32;
-                    const uint32_t boff = (kk >> 2) * (64 * 128) + (kk & 3) * 32;
-                    const uint64_t da = make_sdesc(pa[prod] + aoff, 1024);
-                    const uint64_t db = make_sdesc(pb[prod] + boff, 1024);
-                    const uint32_t acc = (prod | kk) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
-                            tmem),
-                        "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
-                        : "memory");
-                }
-            }
-            asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    bar_mma)
-                : "memory");
-        }
-        if (!tc_wait(bar_mma, mma_phase)) {
-            // give the tensor-core work in flight a second bounded wait before
-            // the accumulator columns are released below
-            tc_wait(bar_mma, mma_phase);
-            ok = false;
-            break;
-        }
-        mma_phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // D rows back: warp w owns TMEM lanes 32w..32w+31; thread = row tid
-        {
-            float d[64];
+            for (int j = 0; j < 7; ++j) lbase |= (((uint32_t)tid >> j) & 1u) << blk.row_bits[j];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + q * 16;
-                uint32_t r[16];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, "
-                    "%8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                      "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                      "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                    : "r"(taddr));
+                float hi[16], lo[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) d[q * 16 + i] = __uint_as_float(r[i]);
+                for (int c = 0; c < 8; ++c) {
+                    const uint32_t l = lbase | blocks[bi].col_bits[q * 8 + c];
+                    const float2 v = *(const float2 *)(tile + tile_off(l));
+                    const float rh = to_tf32(v.x), ih = to_tf32(v.y);
+                    hi[2 * c] = rh;
+                    hi[2 * c + 1] = ih;
+                    lo[2 * c] = to_tf32(v.x - rh);
+                    lo[2 * c + 1] = to_tf32(v.y - ih);
+                }
+                tmem_st16(lane_base + kColAh + q * 16, hi);
+                tmem_st16(lane_base + kColAl + q * 16, lo);
             }
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const uint32_t m = tid;
-            uint32_t lbase = 0;
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (tid == 0) {
+                if (!tc_wait(bar_b, b_phase)) {
+                    atomicExch(s_abort, 1);
+                } else {
+                    const uint32_t bh = tc_smem_u32(b_hi), bl = tc_smem_u32(b_lo);
 #pragma unroll
-            for (int j = 0; j < 7; ++j) lbase |= ((m >> j) & 1u) << blk.row_bits[j];
+                    for (int prod = 0; prod < 3; ++prod) {
+                        // hi.Bhi + hi.Blo + lo.Bhi
+                        const uint32_t acol = prod == 2 ? kColAl : kColAh;
+                        const uint32_t bsrc = prod == 1 ? bl : bh;
 #pragma unroll
-            for (uint32_t c = 0; c < 32; ++c) {
-                uint32_t l = lbase;
-#pragma unroll
-                for (int j = 0; j < 5; ++j) l |= ((c >> j) & 1u) << blk.k[j];
-                *(float2 *)(tile + tile_off(l)) = make_float2(d[2 * c], d[2 * c + 1]);
+                        for (int kk = 0; kk < 8; ++kk) {
+                            const uint32_t boff = (kk >> 2) * (64 * 128) + (kk & 3) * 32;
+                            const uint64_t db = make_sdesc(bsrc + boff, 1024);
+                            const uint32_t acc = (prod | kk) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::
+                                    "r"(tmem + kColD),
+                                "r"(tmem + acol + kk * 8), "l"(db), "r"(kIdesc), "r"(acc)
+                                : "memory");
+                        }
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                        "[%0];" ::"r"(bar_mma)
+                        : "memory");
+                    mma_pending = true;
+                }
+                b_phase ^= 1u;
             }
+            __syncthreads();
+            if (*s_abort) break;
+            // every thread decides to stop only after the barrier, so the CTA
+            // leaves the loop together
+            if (!tc_wait(bar_mma, mma_phase)) atomicExch(s_abort, 1);
+            __syncthreads();
+            if (*s_abort) break;
+            mma_phase ^= 1u;
+            if (tid == 0) mma_pending = false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // D row m = tid back into the tile
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float d[16];
+                tmem_ld16(lane_base + kColD + q * 16, d);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const uint32_t l = lbase | blocks[bi].col_bits[q * 8 + c];
+                    *(float2 *)(tile + tile_off(l)) = make_float2(d[2 * c], d[2 * c + 1]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        (void)lane;
-    }
-    if (ok) {
+        if (*s_abort) break;
+        // tile -> HBM (asynchronous; waited for before this buffer is reloaded)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
+            const int32_t c1 = t & ((1 << (h - 4)) - 1), c3 = t >> (h - 4);
             asm volatile(
                 "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group"
                 " [%0, {%1, %2, %3, %4}], [%5];" ::"l"((uint64_t)&tmap),
                 "r"(zero), "r"(c1), "r"(zero), "r"(c3), "r"(tile_a)
                 : "memory");
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-            asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
         }
-    } else if (tid == 0) {
-        atomicOr(flag, kFlagTimeout);
+        buf ^= 1;
+    }
+    if (tid == 0) {
+        if (*s_abort) {
+            atomicOr(flag, kFlagTimeout);
+            // let work in flight finish before the CTA's memory is released
+            if (mma_pending) tc_wait(bar_mma, mma_phase);
+            for (int b = 0; b < 2; ++b)
+                if (load_pending[b]) tc_wait(bar_load0 + 8u * b, load_phase[b]);
+        }
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols)
                      : "memory");
 }
 
@@ -328,6 +379,14 @@ static int tc_tile_map(CUtensorMap *map, void *d, int n, int h) {
 }
 
 using cd = std::complex<double>;
+
+// SM count of the current device (persistent grid: two CTAs per SM).
+static int tc_sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(sms, 1);
+}
 
 // Apply canonical op g (global index bits) to a 32-dim vector whose block bit j
 // corresponds to global bit gbit[j].
@@ -536,6 +595,10 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
                 }
             TcBlock tb{};
             for (int j = 0; j < 5; ++j) tb.k[j] = local_pos(gbit[j], st.pass.h);
+            for (int c = 0; c < 32; ++c) {
+                tb.col_bits[c] = 0;
+                for (int j = 0; j < 5; ++j) tb.col_bits[c] |= (uint32_t)((c >> j) & 1) << tb.k[j];
+            }
             int nr = 0;
             for (int l = 0; l < kTcT; ++l) {
                 bool inb = false;
@@ -575,9 +638,10 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
         const TcPass &tp = passes[step_pass[si]];
         CUtensorMap map;
         LQ_TRY(tc_tile_map(&map, s->d, n, tp.h));
+        const int ntiles = 1 << (n - kTcT);
         prof_begin(s->stream, kProfTc);
-        k_tc_pass<<<1u << (n - kTcT), kTcThreads, kTcSmem, s->stream>>>(
-            map, tp.h, tp.h + 8, d_blocks + tp.block_begin, tp.nblocks, d_bimg, s->d_flag);
+        k_tc_pass<<<std::min(ntiles, 2 * tc_sm_count()), kTcThreads, kTcSmem, s->stream>>>(
+            map, tp.h, ntiles, d_blocks + tp.block_begin, tp.nblocks, d_bimg, s->d_flag);
         prof_end(s->stream, kProfTc);
         LQ_CUDA_TRY(cudaGetLastError());
         ++launches;
