@@ -363,6 +363,25 @@ int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits);
 int lq_batch_set_tile_bits(lq_batch *b, int tile_bits);
 
 /* ---------------------------------------------------------------------------
+ * Noise models (NoiseModel::apply, src/noise/mod.rs) on complex128 states.
+ * As in the reference, `qubit` here is the basis-index bit (1 << qubit), not
+ * the gate convention n-1-qubit; `qubits` NULL means every qubit.
+ * ------------------------------------------------------------------------- */
+/* apply_x_error / apply_y_error / apply_z_error (src/noise/mod.rs:337-380):
+ * pauli 1 = X, 2 = Y (the reference's -Y), 3 = Z.  DepolarizingNoise
+ * (src/noise/mod.rs:60-83) draws its errors on the host and calls this. */
+int lq_noise_pauli(lq_state *s, int qubit, int pauli);
+/* AmplitudeDampingNoise::apply (src/noise/mod.rs:108-146): the sum over target
+ * qubits of (K0 + K1) psi, K0 = |0><0| + sqrt(1-g)|1><1|, K1 = sqrt(g)|0><1|,
+ * then normalised.  More than one target needs a scratch vector of 2^n
+ * amplitudes (LQ_ERR_OOM if it cannot be allocated). */
+int lq_noise_amplitude_damping(lq_state *s, double gamma, const int *qubits, int nqubits);
+/* PhaseDampingNoise::apply (src/noise/mod.rs:173-210): |1> amplitudes of the
+ * LAST target qubit scaled by sqrt(1-lambda) (each target rewrites the
+ * vector), then normalised. */
+int lq_noise_phase_damping(lq_state *s, double lambda, const int *qubits, int nqubits);
+
+/* ---------------------------------------------------------------------------
  * Learned warm start.  No reference counterpart: the reference starts every
  * VQE from caller-supplied angles (VQE::run, src/optimization/vqe.rs:69-88);
  * these calls produce such angles.  A fully connected network in FP32 on the

@@ -26,6 +26,7 @@ SOURCES = [
     "batch.cu",
     "tc.cu",
     "learned.cu",
+    "noise.cu",
 ]
 
 NVCC_FLAGS = [

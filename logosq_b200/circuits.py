@@ -50,6 +50,7 @@ class Circuit:
         self._ops: list[Operation] = []
         self._name: str | None = None
         self._packed: np.ndarray | None = None
+        self._noise: list = []
 
     # -- metadata ---------------------------------------------------------
     def with_name(self, name: str) -> "Circuit":
@@ -236,11 +237,21 @@ class Circuit:
         return self._packed
 
     # -- execution (src/circuits/mod.rs:196-375) --------------------------
-    def execute(self, state, theta=None, mode: int = abi.EXEC_FUSED) -> None:
+    def add_noise(self, noise_model) -> "Circuit":
+        """Circuit::add_noise (src/circuits/mod.rs:340-343)."""
+        self._noise.append(noise_model)
+        return self
+
+    def _check_state(self, state):
         if state.num_qubits() != self._n:
             raise LogosQError(abi.LQ_ERR_QUBIT_MISMATCH,
                               f"Circuit qubit count mismatch: circuit has {self._n}, "
                               f"state has {state.num_qubits()}")
+
+    def execute_without_noise(self, state, theta=None, mode: int = abi.EXEC_FUSED) -> None:
+        """Circuit::execute_without_noise (src/circuits/mod.rs:196-209), one
+        fused launch sequence for the whole circuit."""
+        self._check_state(state)
         th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float64)
         nth = 0 if th is None else len(th)
         thp = None if th is None else abi.f64_ptr(th)
@@ -251,7 +262,24 @@ class Circuit:
                 call("lq_apply_circuit", state.handle, self._n, abi.gate_ptr(seg), len(seg),
                      thp, nth, mode)
 
-    execute_without_noise = execute
+    def execute(self, state, theta=None, mode: int = abi.EXEC_FUSED) -> None:
+        """Circuit::execute (src/circuits/mod.rs:352-375): without noise models
+        the whole circuit runs fused; with them, every gate is followed by every
+        noise model, in order."""
+        if not self._noise:
+            return self.execute_without_noise(state, theta, mode)
+        self._check_state(state)
+        th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float64)
+        nth = 0 if th is None else len(th)
+        thp = None if th is None else abi.f64_ptr(th)
+        for op in self._ops:
+            if op.dense is not None:
+                MatrixGate(op.dense).apply(state)
+            else:
+                call("lq_apply_circuit", state.handle, self._n, abi.gate_ptr(op.desc), 1, thp,
+                     nth, abi.EXEC_PER_GATE)
+            for model in self._noise:
+                model.apply(state)
 
     def last_stats(self, state):
         launches, passes = C.c_int(), C.c_int()

@@ -12,6 +12,7 @@ reference's tests/*.rs) and against numpy; see logosq_oracle.cpp's header.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import subprocess
 from pathlib import Path
 
@@ -231,3 +232,45 @@ def dense_hamiltonian(n: int, terms: np.ndarray) -> np.ndarray:
         phase = -1.0 if ny % 4 == 2 else 1.0
         H[idx ^ x, idx] += float(t["coefficient"]) * phase * (1.0 - 2.0 * parity)
     return H
+
+
+# ---------------------------------------------------------------------------
+# Noise models: numpy restatement of src/noise/mod.rs (bit `qubit` = 1 << qubit)
+# ---------------------------------------------------------------------------
+def noise_pauli(psi, qubit: int, pauli: int):
+    """apply_x_error / apply_y_error / apply_z_error (src/noise/mod.rs:337-380)."""
+    idx = np.arange(len(psi))
+    j = idx ^ (1 << qubit)
+    bit = (idx >> qubit) & 1
+    if pauli == 1:
+        return psi[j].copy()
+    if pauli == 2:  # new[i] = -i psi[j] if bit(i) else +i psi[j]
+        return np.where(bit == 1, -1j, 1j) * psi[j]
+    return np.where(bit == 1, -psi, psi)
+
+
+def noise_amplitude_damping(psi, gamma: float, qubits):
+    """AmplitudeDampingNoise::apply (src/noise/mod.rs:108-146): one zero vector,
+    every target qubit's K0 + K1 terms added into it, then normalised."""
+    new = np.zeros_like(psi)
+    idx = np.arange(len(psi))
+    for q in qubits:
+        bit = (idx >> q) & 1
+        zero = bit == 0
+        new[zero] += psi[zero]
+        one = ~zero
+        new[one] += psi[one] * math.sqrt(1.0 - gamma)
+        np.add.at(new, idx[one] & ~(1 << q), psi[one] * math.sqrt(gamma))
+    return new / np.sqrt(np.sum(np.abs(new) ** 2))
+
+
+def noise_phase_damping(psi, lam: float, qubits):
+    """PhaseDampingNoise::apply (src/noise/mod.rs:173-210): each target qubit
+    rewrites the vector from the input, so the last one's damping survives;
+    then normalised."""
+    idx = np.arange(len(psi))
+    new = psi.copy()
+    for q in qubits:
+        new = psi.copy()
+        new[((idx >> q) & 1) == 1] *= math.sqrt(1.0 - lam)
+    return new / np.sqrt(np.sum(np.abs(new) ** 2))
