@@ -428,6 +428,15 @@ def run_learned(args):
                                         "batched_wall_s": batched_wall(k, t),
                                         "plain_wall_s": plain_wall(k, t)} for t in tols},
             "batched_s_per_iteration": sec[k]}
+    # Same-quality comparison: iterations until a start reaches the energy that
+    # random-init VQE ends at after eval_iters iterations (+1e-3).
+    r_final = traces["random"][:, -1]
+    match = {}
+    for k, tr in traces.items():
+        it = learned.iterations_to(tr, r_final, 1e-3)
+        match[k] = {"median_iters": float(np.median(it)),
+                    "reached_frac": float(np.mean(it < cap)),
+                    "frac_ending_below_random": float(np.mean(tr[:, -1] < r_final - 1e-9))}
     tol = 1e-3
     plain_random = plain_wall("random", tol)
     batched_random = batched_wall("random", tol)
@@ -458,6 +467,7 @@ def run_learned(args):
             "warm_batched_wall_s_to_target": warm_batched,
             "plain_s_per_iteration_by_qubits": t_plain,
             "starts": summary,
+            "to_random_init_final_energy": match,
             "exact": {"min_gap_best_to_E0": float((best - E0).min()),
                       "median_gap_best_to_E0": float(np.median(best - E0)),
                       "frac_within_1e-3_of_E0": float(np.mean(best - E0 < 1e-3)),
