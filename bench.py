@@ -329,6 +329,67 @@ def run_precision(args):
     return 0
 
 
+def run_qft(args):
+    """Plain QFT (qft::create_circuit, src/algorithms/qft.rs:10-27) on a seeded
+    complex Gaussian state: effective GB/s of the fused and per-gate paths (the
+    algorithmic bytes of workloads.qft_bytes over device time; a 20-qubit state
+    is 16 MiB, so it lives in L2), max-abs error against the oracle, and the
+    oracle's serial run on the host beside it."""
+    import torch
+    import oracle
+    from logosq_b200 import State, abi, workloads
+    from logosq_b200._lib import call
+
+    n = args.qubits if args.qubits != 30 else 20
+    v = workloads.gaussian_state(n, 1)
+    g = workloads.qft_gates(n)
+    st = State.zero_state(n)
+    sp = C.c_void_p()
+    call("lq_state_stream", st.handle, C.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value)
+    res = {}
+    for name, mode in (("fused", abi.EXEC_FUSED), ("per_gate", abi.EXEC_PER_GATE)):
+        for _ in range(args.warmup):
+            st.set_vector(v)
+            call("lq_apply_circuit", st.handle, n, abi.gate_ptr(g), len(g), None, 0, mode)
+        st.synchronize()
+        ms = 0.0
+        for _ in range(args.steps):
+            st.set_vector(v)
+            st.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call("lq_apply_circuit", st.handle, n, abi.gate_ptr(g), len(g), None, 0, mode)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        res[name] = ms / args.steps
+    got = st.vector()
+    st.close()
+    oracle.set_threads(1)
+    t0 = time.perf_counter()
+    want = oracle.apply_circuit(v.copy(), g)
+    cpu_s = time.perf_counter() - t0
+    algo = workloads.qft_bytes(n)
+    line = {"metric": f"{n}q QFT effective GB/s", "value": algo / (res["fused"] / 1e3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["fused"], "higher_is_better": True, "vs_baseline": None,
+            "dtype": "f64 (complex128)", "data": "synthetic (seeded)",
+            "config": {"workload": f"QFT on a seeded complex Gaussian {n}-qubit state "
+                                   f"({len(g)} gates)", "algorithmic_bytes": algo,
+                       "l2_policy": "state fits L2 (16 MiB at 20 qubits)"},
+            "per_gate_path": {"value": algo / (res["per_gate"] / 1e3) / 1e9, "unit": "GB/s",
+                              "ms_per_step": res["per_gate"]},
+            "max_abs_error_vs_oracle": float(np.abs(got - want).max()),
+            "cpu_baseline": {"value": algo / cpu_s / 1e9, "unit": "GB/s", "cores": 1,
+                             "kind": "port", "sample": f"the whole {n}-qubit QFT, serial "
+                                                       f"restatement of the reference loops, "
+                                                       f"{cpu_s:.2f} s"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_learned(args):
     """Learned form: disordered XYZ chains (n 12-16 by default).  Train the
     warm-start network on batched-VQE optima (fixed small-angle start), then on
@@ -506,7 +567,7 @@ def main():
     ap.add_argument("--fusion-width", type=int, default=0,
                     help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
     ap.add_argument("--workload", default="brickwork",
-                    choices=["brickwork", "vqe-batch", "precision", "learned"])
+                    choices=["brickwork", "vqe-batch", "precision", "learned", "qft"])
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--check-qubits", type=int, default=30,
                     help="precision form: qubit count of the comparison against complex128 "
@@ -530,6 +591,8 @@ def main():
         return run_precision(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "qft":
+        return run_qft(args)
     n, layers = args.qubits, args.layers
     ws, rank, local = dist_info()
     metric = f"{n}q gate-layer GB/s"

@@ -17,7 +17,8 @@ from .circuits import Circuit, Operation
 from .optimization import (Pauli, PauliTerm, PauliObservable, Observable, Ansatz,
                            HardwareEfficientAnsatz, RealAmplitudesAnsatz, EfficientSU2Ansatz,
                            ParameterizedCircuit, EntanglingGate, EntanglingPattern,
-                           ParameterShift, FiniteDifference, GradientDescent, Adam, VQE)
+                           ParameterShift, FiniteDifference, GradientDescent, Adam, VQE,
+                           QuantumNaturalGradient)
 from .algorithms import qft, rqc, xyz_heisenberg
 from .qml import VariationalQuantumCircuit, VQCType
 
@@ -26,6 +27,7 @@ __all__ = [
     "Operation", "Pauli", "PauliTerm", "PauliObservable", "Observable", "Ansatz",
     "HardwareEfficientAnsatz", "RealAmplitudesAnsatz", "EfficientSU2Ansatz",
     "ParameterizedCircuit", "EntanglingGate", "EntanglingPattern", "ParameterShift",
-    "FiniteDifference", "GradientDescent", "Adam", "VQE", "qft", "rqc", "xyz_heisenberg",
+    "FiniteDifference", "GradientDescent", "Adam", "VQE", "QuantumNaturalGradient",
+    "qft", "rqc", "xyz_heisenberg",
     "VariationalQuantumCircuit", "VQCType",
 ]

@@ -570,7 +570,11 @@ int lq_lanczos_ground_energy(int num_qubits, const lq_pauli_term *terms, int nte
         return set_error(e == cudaErrorMemoryAllocation ? LQ_ERR_OOM : LQ_ERR_CUDA, "%s",
                          cudaGetErrorString(e));
     }
-    cudaMemcpy(dterms, rt.data(), sizeof(RealTerm) * rt.size(), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(dterms, rt.data(), sizeof(RealTerm) * rt.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cleanup();
+        return set_error(LQ_ERR_CUDA, "%s", cudaGetErrorString(e));
+    }
     {  // seeded random start vector (host), normalised
         std::vector<double> v0(N);
         std::mt19937_64 rng(seed);
@@ -582,15 +586,24 @@ int lq_lanczos_ground_energy(int num_qubits, const lq_pauli_term *terms, int nte
         }
         s = 1.0 / std::sqrt(s);
         for (auto &x : v0) x *= s;
-        cudaMemcpy(V, v0.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+        if ((e = cudaMemcpy(V, v0.data(), sizeof(double) * N, cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+            cleanup();
+            return set_error(LQ_ERR_CUDA, "%s", cudaGetErrorString(e));
+        }
     }
     // <V_j, x> for j < count, block partials summed on the host in a fixed order.
     std::vector<double> hpart((size_t)kDotBlocks * (kmax + 1)), hc(kmax + 1);
+    cudaError_t err = cudaSuccess;  // first failure of any launch or copy below
+    auto note = [&](cudaError_t r) {
+        if (err == cudaSuccess && r != cudaSuccess) err = r;
+    };
     auto dots = [&](const double *Vb, int count, const double *x) {
         k_multi_dot<<<dim3(kDotBlocks, count), 256, 0, st>>>(Vb, x, N, part);
-        cudaMemcpyAsync(hpart.data(), part, sizeof(double) * kDotBlocks * count,
-                        cudaMemcpyDeviceToHost, st);
-        cudaStreamSynchronize(st);
+        note(cudaGetLastError());
+        note(cudaMemcpyAsync(hpart.data(), part, sizeof(double) * kDotBlocks * count,
+                             cudaMemcpyDeviceToHost, st));
+        note(cudaStreamSynchronize(st));
         for (int j = 0; j < count; ++j) {
             double s = 0.0;
             for (int b = 0; b < kDotBlocks; ++b) s += hpart[(size_t)j * kDotBlocks + b];
@@ -613,11 +626,13 @@ int lq_lanczos_ground_energy(int num_qubits, const lq_pauli_term *terms, int nte
         // full reorthogonalisation against V_0..V_k, classical Gram-Schmidt twice
         for (int pass = 0; pass < 2; ++pass) {
             dots(V, k + 1, w);
-            cudaMemcpyAsync(coef, hc.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, st);
+            note(cudaMemcpyAsync(coef, hc.data(), sizeof(double) * (k + 1),
+                                 cudaMemcpyHostToDevice, st));
             k_multi_sub<<<grid, 256, 0, st>>>(V, coef, k + 1, N, w);
         }
         dots(w, 1, w);
         const double b = std::sqrt(std::max(hc[0], 0.0));
+        if (err != cudaSuccess) break;
         ev = tridiag_min_eig(alpha, beta);
         if (std::fabs(ev - prev) < tol || b < 1e-12) {
             ++k;
@@ -629,6 +644,7 @@ int lq_lanczos_ground_energy(int num_qubits, const lq_pauli_term *terms, int nte
     }
     e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = err;
     cleanup();
     if (e != cudaSuccess) return set_error(LQ_ERR_CUDA, "%s", cudaGetErrorString(e));
     *e0 = ev;

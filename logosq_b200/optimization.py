@@ -586,3 +586,77 @@ class VQE:
         rng = np.random.default_rng(seed)
         init = rng.uniform(0.0, 2.0 * math.pi, self.ansatz.num_parameters())
         return self.run(init)
+
+
+# ---------------------------------------------------------------------------
+# Quantum natural gradient (src/optimization/qng.rs)
+# ---------------------------------------------------------------------------
+class QuantumNaturalGradient:
+    """QuantumNaturalGradient (src/optimization/qng.rs:12-141) on the device.
+
+    compute_metric_tensor follows the reference's formula (qng.rs:29-87): for
+    every pair i <= j the four states with parameters i, j shifted by
+    (+s, +s), (+s, -s), (-s, +s), (-s, -s), s = pi/2, are prepared by the
+    engine and
+        g_ij = (|<pp|pp>| - |<pp|pm>| - |<mp|pp>| + |<mm|mm>|) / 8,
+    symmetric, plus `regularization` on the diagonal.  States for a parameter
+    vector that occurs more than once are prepared once.
+    compute_natural_gradient returns the plain gradient, as the reference does:
+    its linear solve is a placeholder that returns the right-hand side
+    (qng.rs:117-134)."""
+
+    def __init__(self, regularization: float = 1e-8):
+        self.regularization = float(regularization)
+
+    @classmethod
+    def with_regularization(cls, regularization: float) -> "QuantumNaturalGradient":
+        return cls(regularization)
+
+    def compute_metric_tensor(self, ansatz, parameters) -> np.ndarray:
+        p = np.asarray(parameters, dtype=np.float64)
+        n = len(p)
+        shift = math.pi / 2.0
+        cache: dict = {}
+
+        def state_for(vec):
+            key = vec.tobytes()
+            st = cache.get(key)
+            if st is None:
+                st = State.zero_state(ansatz.num_qubits())
+                ansatz.apply(st, vec)
+                cache[key] = st
+            return st
+
+        metric = np.zeros((n, n))
+        try:
+            for i in range(n):
+                for j in range(i, n):
+                    vecs = []
+                    for si, sj in ((1, 1), (1, -1), (-1, 1), (-1, -1)):
+                        v = p.copy()
+                        v[i] += si * shift
+                        v[j] += sj * shift
+                        vecs.append(v)
+                    pp, pm, mp, mm = (state_for(v) for v in vecs)
+                    o_pp = abs(pp.inner_product(pp))
+                    o_pm = abs(pp.inner_product(pm))
+                    o_mp = abs(mp.inner_product(pp))
+                    o_mm = abs(mm.inner_product(mm))
+                    g = (o_pp - o_pm - o_mp + o_mm) / 8.0
+                    metric[i, j] = g
+                    metric[j, i] = g
+                # states of row i are not needed again once j has passed them
+                if len(cache) > 4 * (n + 1):
+                    for st in cache.values():
+                        st.close()
+                    cache.clear()
+        finally:
+            for st in cache.values():
+                st.close()
+        metric[np.diag_indices(n)] += self.regularization
+        return metric
+
+    def compute_natural_gradient(self, ansatz, observable, gradient_method, parameters):
+        gradient = np.asarray(gradient_method.compute_gradient(ansatz, observable, parameters))
+        self.compute_metric_tensor(ansatz, parameters)
+        return gradient
