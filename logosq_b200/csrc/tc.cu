@@ -599,12 +599,34 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
                 tb.col_bits[c] = 0;
                 for (int j = 0; j < 5; ++j) tb.col_bits[c] |= (uint32_t)((c >> j) & 1) << tb.k[j];
             }
-            int nr = 0;
+            // Row bits: thread m's bit j goes to tile bit row_bits[j].  The row order
+            // is free (each thread writes back the row it read), so the five lane
+            // bits (j < 5) take tile bits whose 8-byte bank slots in the swizzled
+            // tile are linearly independent: slot(l) = (l0, l1^l4, l2^l5, l3^l6), so
+            // tile bit b moves slot bit (b < 4 ? b : b - 3) for b < 7 and none above.
+            // Up to 16 distinct slots per warp access = the two-wavefront minimum.
+            std::vector<int> free_bits;
             for (int l = 0; l < kTcT; ++l) {
                 bool inb = false;
                 for (int j = 0; j < 5; ++j) inb |= tb.k[j] == l;
-                if (!inb) tb.row_bits[nr++] = l;
+                if (!inb) free_bits.push_back(l);
             }
+            auto slot_vec = [](int b) { return b < 7 ? 1u << (b < 4 ? b : b - 3) : 0u; };
+            std::vector<int> order;
+            std::vector<uint32_t> basis;  // reduced slot vectors of the chosen lane bits
+            for (int b : free_bits) {
+                uint32_t v = slot_vec(b);
+                for (uint32_t e : basis)
+                    if ((v ^ e) < v) v ^= e;
+                if (v && order.size() < 5) {
+                    basis.push_back(v);
+                    std::sort(basis.rbegin(), basis.rend());
+                    order.push_back(b);
+                }
+            }
+            for (int b : free_bits)
+                if (std::find(order.begin(), order.end(), b) == order.end()) order.push_back(b);
+            for (int j = 0; j < 7; ++j) tb.row_bits[j] = (uint32_t)order[j];
             tb.b_offset = bimg.size();
             bimg.resize(bimg.size() + 2 * kBBytes);
             write_b_image(W, bimg.data() + tb.b_offset, bimg.data() + tb.b_offset + kBBytes);
