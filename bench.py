@@ -410,8 +410,10 @@ def run_learned(args):
     hist = net.fit(X, T, M, epochs=args.epochs, batch=256, lr=1e-3, val_frac=0.1)
     t_fit = time.perf_counter() - t0
     p_sup = net.params()
+    # the energy stage needs no optima: it also sees fresh chains, for generalisation
+    extra = workloads.disordered_chains(args.energy_extra_chains, seed=7, n_lo=lo, n_hi=hi)
     t0 = time.perf_counter()
-    eh = net.energy_train(train, args.energy_steps, lr=3e-4)
+    eh = net.energy_train(train + extra, args.energy_steps, lr=args.energy_lr)
     t_energy = time.perf_counter() - t0
 
     ev = workloads.disordered_chains(args.eval_chains, seed=6, n_lo=lo, n_hi=hi)
@@ -513,6 +515,8 @@ def run_learned(args):
                                    "L=4, Adam lr 0.05",
                        "train_chains": len(train), "train_vqe_iters": args.vqe_iters,
                        "supervised_epochs": args.epochs, "energy_steps": args.energy_steps,
+                       "energy_lr": args.energy_lr,
+                       "energy_chains": len(train) + args.energy_extra_chains,
                        "eval_chains": len(ev), "eval_iters": iters, "target_tol": tol,
                        "target": "E* = the lowest energy any of the four starts reached for "
                                  "the chain (the exact E0 is out of the ansatz's reach, see "
@@ -575,7 +579,10 @@ def main():
     ap.add_argument("--train-chains", type=int, default=1024)
     ap.add_argument("--vqe-iters", type=int, default=150)
     ap.add_argument("--epochs", type=int, default=200)
-    ap.add_argument("--energy-steps", type=int, default=300)
+    ap.add_argument("--energy-steps", type=int, default=1000)
+    ap.add_argument("--energy-lr", type=float, default=1e-3)
+    ap.add_argument("--energy-extra-chains", type=int, default=1024,
+                    help="learned form: fresh chains added to the energy stage")
     ap.add_argument("--eval-chains", type=int, default=256)
     ap.add_argument("--eval-iters", type=int, default=300)
     ap.add_argument("--save-traces", default=None,
