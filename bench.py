@@ -11,7 +11,7 @@ read and one write of the state per launch).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: the dense single-state simulation does not shard in this build;
+Multi-GPU: the dense single-state simulation is not sharded across GPUs;
 `--gpus N` (under torchrun) runs N independent replicas, one per GPU, and
 reports the whole-job aggregate (weak scaling, no data-path collective).
 """
