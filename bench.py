@@ -390,6 +390,130 @@ def run_qft(args):
     return 0
 
 
+def run_kernels(args):
+    """Each primitive kernel of the per-gate and observable paths on its own, on an
+    n-qubit complex128 state (default 28 qubits: 4 GiB, far larger than L2, so
+    no flush is needed between launches): device time per call from CUDA events
+    recorded around the launches on the state's stream (the engine's launch
+    profiler), the kernel's algorithmic bytes, GB/s and the fraction of the HBM
+    peak.  Algorithmic bytes, S = 16 * 2^n: a 2x2, 4x4 or 16x16 gate or a
+    dense diagonal reads and writes the state (2S); a controlled gate the
+    control = 1 half (S); CPhase the |11> quarter (S/2); SWAP the |01>, |10>
+    half (S); a reduction reads the state once per pass (S; two states for an
+    inner product)."""
+    import torch
+    from logosq_b200 import State, abi
+    from logosq_b200._lib import call
+
+    n = args.qubits if args.qubits != 30 else 28
+    S = 16 << n
+    peak, peak_kind = hbm_peak()
+    rng = np.random.default_rng(11)
+
+    def unitary(d):
+        q, r = np.linalg.qr(rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d)))
+        u = q * (np.diag(r) / np.abs(np.diag(r)))
+        return np.ascontiguousarray(np.stack([u.real, u.imag], -1).reshape(-1))
+
+    def gate(kind, qs, angles=()):
+        g = abi.empty_gates(1)
+        g[0]["kind"] = kind
+        for i, q in enumerate(qs):
+            g[0]["q"][i] = q
+        for i, a in enumerate(angles):
+            g[0]["angle"][i] = a
+        return g
+
+    st = State.plus_state(n)
+    other = State.plus_state(n)
+    out2 = (C.c_double * 2)()
+    out1 = C.c_double()
+    zstring = np.zeros(1, dtype=abi.TERM_DTYPE)
+    zstring[0]["coefficient"] = 1.0
+    zstring[0]["zmask"] = (1 << n) - 1
+    from logosq_b200 import workloads
+    jrng = workloads.uniform_stream(12, 3 * (n - 1) + 1, -1.0, 1.0)
+    heis = workloads.heisenberg_terms(n, jrng[0:n - 1], jrng[n - 1:2 * (n - 1)],
+                                      jrng[2 * (n - 1):3 * (n - 1)], 0.5 * jrng[-1])
+    heis_groups = len({int(x) for x in heis["xmask"]})
+    m2 = unitary(4)
+    m4 = unitary(16)
+    q4 = (C.c_int * 4)(0, n // 3, 2 * n // 3, n - 1)
+    PROF_GATE, PROF_REDUCE, PROF_FUSED = 1, 2, 0
+
+    def apply(g):
+        return lambda: call("lq_apply_gate", st.handle, abi.gate_ptr(g), None, 0)
+
+    u3 = (1.1, 0.7, 2.3)
+    cases = [
+        ("k_1q_shfl", f"U3 on qubit {n - 1} (state bit 0: warp-shuffle pairs)",
+         apply(gate(abi.U3, [n - 1], u3)), 2 * S, PROF_GATE),
+        ("k_1q_pair", "U3 on qubit 0 (top state bit: 128-bit amplitude pairs)",
+         apply(gate(abi.U3, [0], u3)), 2 * S, PROF_GATE),
+        ("k_1q_pair", f"H on qubit {n // 2}", apply(gate(abi.H, [n // 2])), 2 * S, PROF_GATE),
+        ("k_ctrl1q<permutation>", f"CNOT({n // 2}, {n // 2 + 1})",
+         apply(gate(abi.CNOT, [n // 2, n // 2 + 1])), S, PROF_GATE),
+        ("k_ctrl1q", "CRY(3, 7)", apply(gate(abi.CRY, [3, 7], (0.9,))), S, PROF_GATE),
+        ("k_diag", "RZ on qubit 3", apply(gate(abi.RZ, [3], (0.4,))), 2 * S, PROF_GATE),
+        ("k_diag", f"CPhase(2, {n - 3})", apply(gate(abi.CPHASE, [2, n - 3], (0.3,))), S // 2,
+         PROF_GATE),
+        ("k_swap", f"SWAP(1, {n - 2})", lambda: call("lq_apply_swap", st.handle, 1, n - 2),
+         S, PROF_GATE),
+        ("k_2q", "dense 4x4 on qubits (4, 9)",
+         lambda: call("lq_apply_matrix2", st.handle, 4, 9, abi.f64_ptr(m2)), 2 * S, PROF_GATE),
+        ("k_fused_pass (block)", f"dense 16x16 block on qubits {tuple(q4)}",
+         lambda: call("lq_apply_block", st.handle, 4, q4, abi.f64_ptr(m4)), 2 * S, PROF_FUSED),
+        ("k_norm_partial", "norm_sqr", lambda: call("lq_norm_sqr", st.handle, C.byref(out1)),
+         S, PROF_REDUCE),
+        ("k_pauli_group", "one Z-string term",
+         lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(zstring), 1,
+                      abi.Y_REFERENCE, C.byref(out1), None), S, PROF_REDUCE),
+        ("k_pauli_group", f"XYZ chain ({len(heis)} terms, {heis_groups} X-mask groups)",
+         lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(heis), len(heis),
+                      abi.Y_REFERENCE, C.byref(out1), None), heis_groups * S, PROF_REDUCE),
+        ("k_inner_partial", "inner product of two states",
+         lambda: call("lq_inner_product", st.handle, other.handle, out2), 2 * S, PROF_REDUCE),
+    ]
+    dev = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
+    sampler = ClockSampler(dev)
+    rows = []
+    launches = 0
+    sampler.start()
+    for kernel, what, fn, nbytes, cls in cases:
+        for _ in range(args.warmup):
+            fn()
+        st.synchronize()
+        call("lq_profile_enable", 1)
+        for _ in range(args.steps):
+            fn()
+        st.synchronize()
+        tot, cnt = C.c_double(), C.c_longlong()
+        call("lq_profile_read", cls, C.byref(tot), C.byref(cnt))
+        call("lq_profile_enable", 0)
+        ms = tot.value / max(cnt.value, 1)
+        gbs = nbytes / (ms / 1e3) / 1e9
+        launches += cnt.value
+        rows.append({"kernel": kernel, "op": what, "ms": round(ms, 4),
+                     "algorithmic_bytes": nbytes, "GB/s": round(gbs, 1),
+                     "frac": round(gbs / peak, 3)})
+    clocks = sampler.stop()
+    st.close()
+    other.close()
+    torch.cuda.synchronize()
+    line = {"metric": f"{n}q primitive-kernel GB/s (median over kernels)",
+            "value": statistics.median(r["GB/s"] for r in rows), "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "vs_baseline": None, "dtype": "f64 (complex128)",
+            "data": "synthetic (|+...+> state, fixed angles, seeded random matrices)",
+            "config": {"workload": f"each primitive kernel alone on a {n}-qubit complex128 "
+                                   f"state", "state_bytes": S,
+                       "l2_policy": "state larger than L2 (no flush needed)"},
+            "peak": {"hbm_gbs": peak, "kind": f"of {peak_kind}"},
+            "kernels": rows, "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_learned(args):
     """Learned form: disordered XYZ chains (n 12-16 by default).  Train the
     warm-start network on batched-VQE optima (fixed small-angle start), then on
@@ -571,7 +695,7 @@ def main():
     ap.add_argument("--fusion-width", type=int, default=0,
                     help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
     ap.add_argument("--workload", default="brickwork",
-                    choices=["brickwork", "vqe-batch", "precision", "learned", "qft"])
+                    choices=["brickwork", "vqe-batch", "precision", "learned", "qft", "kernels"])
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--check-qubits", type=int, default=30,
                     help="precision form: qubit count of the comparison against complex128 "
@@ -600,6 +724,8 @@ def main():
         return run_learned(args)
     if args.workload == "qft":
         return run_qft(args)
+    if args.workload == "kernels":
+        return run_kernels(args)
     n, layers = args.qubits, args.layers
     ws, rank, local = dist_info()
     metric = f"{n}q gate-layer GB/s"

@@ -166,8 +166,11 @@ int lq_set_alloc_limit(uint64_t bytes);
 /* Launch timing (no reference counterpart; used by the benchmark): when
  * enabled, CUDA events bracket every launch and lq_profile_read returns the
  * summed device time and launch count of one kernel class:
- * 0 fused block passes, 1 per-gate sweeps, 2 reductions, 3 batched engine,
- * 4 tensor-core blocks.  Enabling (or disabling) resets the counters. */
+ * 0 fused block passes, 1 per-gate sweeps, 2 reductions (norm, Pauli-sum
+ * expectation, inner product), 3 batched engine, 4 tensor-core blocks.  One
+ * bracket per call: work a call runs inside another bracket (the norm pass of
+ * a renormalising gate) counts toward the outer class.  Enabling (or
+ * disabling) resets the counters. */
 int lq_profile_enable(int on);
 int lq_profile_read(int kernel_class, double *total_ms, long long *launches);
 

@@ -315,11 +315,13 @@ static int grid_for(uint64_t N, int threads) {
 static int norm_sqr_device(const lq_state *s, double *d_out) {
     const uint64_t N = 1ull << s->n;
     const int th = 256, g = red_grid(N, th);
+    prof_begin(s->stream, kProfReduce);
     if (s->dtype == LQ_C128)
         k_norm_partial<<<g, th, 0, s->stream>>>((const double2 *)s->d, N, s->d_red);
     else
         k_norm_partial<<<g, th, 0, s->stream>>>((const float2 *)s->d, N, s->d_red);
     k_final_sum<1><<<1, 256, 0, s->stream>>>(s->d_red, g, d_out);
+    prof_end(s->stream, kProfReduce);
     LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
 }
@@ -400,6 +402,7 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
     if (!packed.empty())
         LQ_CUDA_TRY(cudaMemcpyAsync(d_tc, packed.data(), coef_bytes, cudaMemcpyHostToDevice,
                                     s->stream));
+    prof_begin(s->stream, kProfReduce);
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const int nt = (int)groups[gi].second.size();
         const size_t shm = nt * sizeof(TermCoef);
@@ -411,6 +414,7 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
                                                      d_tc + offs[gi], nt, s->d_red);
         k_final_sum<1><<<1, 256, 0, s->stream>>>(s->d_red, g, d_res + gi);
     }
+    prof_end(s->stream, kProfReduce);
     LQ_CUDA_TRY(cudaGetLastError());
     std::vector<double> res(groups.size());
     if (!groups.empty())
@@ -916,6 +920,7 @@ int lq_inner_product(const lq_state *a, const lq_state *b, double out[2]) {
     const uint64_t N = 1ull << a->n;
     const int th = 256, g = red_grid(N, th);
     double *d_out = ma->d_red + kRedBlocks * 2 * kMaxTermsPerPass - 4;
+    prof_begin(a->stream, kProfReduce);
     if (a->dtype == LQ_C128)
         k_inner_partial<<<g, th, 0, a->stream>>>((const double2 *)a->d, (const double2 *)b->d, N,
                                                  ma->d_red);
@@ -923,6 +928,7 @@ int lq_inner_product(const lq_state *a, const lq_state *b, double out[2]) {
         k_inner_partial<<<g, th, 0, a->stream>>>((const float2 *)a->d, (const float2 *)b->d, N,
                                                  ma->d_red);
     k_final_sum<2><<<1, 256, 0, a->stream>>>(ma->d_red, g, d_out);
+    prof_end(a->stream, kProfReduce);
     LQ_CUDA_TRY(cudaGetLastError());
     LQ_CUDA_TRY(cudaMemcpyAsync(ma->h_red, d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                                 a->stream));

@@ -20,6 +20,12 @@ double g_ms[kProfClasses] = {0};
 long g_count[kProfClasses] = {0};
 thread_local cudaEvent_t t_begin = nullptr;
 thread_local int t_cls = -1;
+// Brackets nest (a renormalising gate runs the norm reduction inside its own
+// bracket): only the outermost one records events; inner ones count toward it.
+thread_local int t_depth = 0;
+// Bumped by lq_profile_enable so a bracket left open across a reset is dropped.
+unsigned g_gen = 0;
+thread_local unsigned t_gen = 0;
 
 cudaEvent_t take_event() {
     if (!g_pool.empty()) {
@@ -56,14 +62,23 @@ static bool capturing(cudaStream_t st) {
 void prof_begin(cudaStream_t st, int cls) {
     if (!g_on || capturing(st)) return;
     std::lock_guard<std::mutex> lk(g_mu);
+    if (t_gen != g_gen) {
+        t_gen = g_gen;
+        t_depth = 0;
+        t_begin = nullptr;
+    }
+    if (t_depth++ > 0) return;
     t_begin = take_event();
     t_cls = cls;
     cudaEventRecord(t_begin, st);
 }
 
 void prof_end(cudaStream_t st, int cls) {
-    if (!g_on || !t_begin || t_cls != cls || capturing(st)) return;
+    if (!g_on || capturing(st)) return;
     std::lock_guard<std::mutex> lk(g_mu);
+    if (t_gen != g_gen || t_depth == 0) return;
+    if (--t_depth > 0) return;
+    if (!t_begin || t_cls != cls) return;
     cudaEvent_t e = take_event();
     cudaEventRecord(e, st);
     g_pending.push_back({cls, t_begin, e});
@@ -81,6 +96,7 @@ int lq_profile_enable(int on) {
     std::lock_guard<std::mutex> lk(g_mu);
     resolve_locked();
     g_on = on != 0;
+    ++g_gen;
     for (int c = 0; c < kProfClasses; ++c) {
         g_ms[c] = 0.0;
         g_count[c] = 0;
