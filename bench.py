@@ -438,7 +438,9 @@ def run_kernels(args):
     heis_groups = len({int(x) for x in heis["xmask"]})
     m2 = unitary(4)
     m4 = unitary(16)
-    q4 = (C.c_int * 4)(0, n // 3, 2 * n // 3, n - 1)
+    # block qubits: bits 2, n-12, n-8, n-5 (the bits above 3 must fit one
+    # 8-bit tile window)
+    q4 = (C.c_int * 4)(n - 3, 11, 7, 4)
     PROF_GATE, PROF_REDUCE, PROF_FUSED = 1, 2, 0
 
     def apply(g):

@@ -428,25 +428,28 @@ int lq_mlp_num_params(const lq_mlp *net, int64_t *out) {
 }
 
 int lq_mlp_get_params(const lq_mlp *net, float *host, int64_t count) {
-    if (!net || !host || count != net->nparams)
+    if (!net || !host) return set_error(LQ_ERR_INVALID_ARG, "null argument");
+    if (count != net->nparams)
         return set_error(LQ_ERR_PARAM_COUNT, "Parameter count mismatch: expected %lld, got %lld",
-                         (long long)(net ? net->nparams : 0), (long long)count);
+                         (long long)net->nparams, (long long)count);
     LQ_CUDA_TRY(cudaMemcpy(host, net->p, count * 4, cudaMemcpyDeviceToHost));
     return LQ_OK;
 }
 
 int lq_mlp_set_params(lq_mlp *net, const float *host, int64_t count) {
-    if (!net || !host || count != net->nparams)
+    if (!net || !host) return set_error(LQ_ERR_INVALID_ARG, "null argument");
+    if (count != net->nparams)
         return set_error(LQ_ERR_PARAM_COUNT, "Parameter count mismatch: expected %lld, got %lld",
-                         (long long)(net ? net->nparams : 0), (long long)count);
+                         (long long)net->nparams, (long long)count);
     LQ_CUDA_TRY(cudaMemcpy(net->p, host, count * 4, cudaMemcpyHostToDevice));
     return LQ_OK;
 }
 
 int lq_mlp_get_grads(const lq_mlp *net, float *host, int64_t count) {
-    if (!net || !host || count != net->nparams)
+    if (!net || !host) return set_error(LQ_ERR_INVALID_ARG, "null argument");
+    if (count != net->nparams)
         return set_error(LQ_ERR_PARAM_COUNT, "Parameter count mismatch: expected %lld, got %lld",
-                         (long long)(net ? net->nparams : 0), (long long)count);
+                         (long long)net->nparams, (long long)count);
     LQ_CUDA_TRY(cudaMemcpy(host, net->g, count * 4, cudaMemcpyDeviceToHost));
     return LQ_OK;
 }
