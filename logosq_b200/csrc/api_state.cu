@@ -350,6 +350,13 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
             return set_error(LQ_ERR_INVALID_ARG,
                              "Pauli term %d: ny=%d but xmask&zmask has %d bits", t, terms[t].ny, ny);
     }
+    // Large states: one sweep per tile window instead of one per X mask.
+    if (!per_term) {
+        bool handled = false;
+        LQ_TRY(expectation_windows(const_cast<lq_state *>(s), terms, nterms, yconv, out,
+                                   &handled));
+        if (handled) return LQ_OK;
+    }
     // Re(Y^ny z) selectors: Y = +i (reference convention) or -i (textbook).
     auto selectors = [&](int ny, double &a, double &b) {
         int k = ny & 3;
