@@ -390,31 +390,6 @@ def run_qft(args):
     return 0
 
 
-def pauli_sweeps(terms, n: int, m: int = 8) -> int:
-    """State sweeps of one Pauli-sum expectation in the engine: for complex128
-    states of 16 or more qubits, one per tile window (bits 0-3 and m consecutive
-    bits), the windows chosen by greedy stabbing of each X-mask group's range of
-    window starts; otherwise one per X-mask group."""
-    xs = sorted({int(x) for x in terms["xmask"]})
-    if n < 16:
-        return len(xs)
-    spans = []
-    for x in xs:
-        hx = x & ~0xF
-        if not hx:
-            continue
-        lb, hb = (hx & -hx).bit_length() - 1, hx.bit_length() - 1
-        lo, hi = max(4, hb - m + 1), min(lb, n - m)
-        if lo > hi:
-            return len(xs)
-        spans.append((hi, lo))
-    count, cur = 0, None
-    for hi, lo in sorted(spans):
-        if cur is None or lo > cur:
-            cur, count = hi, count + 1
-    return max(count, 1)
-
-
 def run_kernels(args):
     """Each primitive kernel of the per-gate and observable paths on its own, on an
     n-qubit complex128 state (default 28 qubits: 4 GiB, far larger than L2, so
@@ -424,8 +399,8 @@ def run_kernels(args):
     peak.  Algorithmic bytes, S = 16 * 2^n: a 2x2, 4x4 or 16x16 gate or a
     dense diagonal reads and writes the state (2S); a controlled gate the
     control = 1 half (S); CPhase the |11> quarter (S/2); SWAP the |01>, |10>
-    half (S); a reduction reads the state once per sweep (S; two states for an
-    inner product; a Pauli sum sweeps once per tile window, pauli_sweeps)."""
+    half (S); a reduction reads the state once per pass (S; two states for an
+    inner product)."""
     import torch
     from logosq_b200 import State, abi
     from logosq_b200._lib import call
@@ -461,7 +436,6 @@ def run_kernels(args):
     heis = workloads.heisenberg_terms(n, jrng[0:n - 1], jrng[n - 1:2 * (n - 1)],
                                       jrng[2 * (n - 1):3 * (n - 1)], 0.5 * jrng[-1])
     heis_groups = len({int(x) for x in heis["xmask"]})
-    heis_sweeps = pauli_sweeps(heis, n)
     m2 = unitary(4)
     m4 = unitary(16)
     # block qubits: bits 2, n-12, n-8, n-5 (the bits above 3 must fit one
@@ -493,13 +467,12 @@ def run_kernels(args):
          lambda: call("lq_apply_block", st.handle, 4, q4, abi.f64_ptr(m4)), 2 * S, PROF_FUSED),
         ("k_norm_partial", "norm_sqr", lambda: call("lq_norm_sqr", st.handle, C.byref(out1)),
          S, PROF_REDUCE),
-        ("k_energy_windows", "one Z-string term",
+        ("k_pauli_group", "one Z-string term",
          lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(zstring), 1,
                       abi.Y_REFERENCE, C.byref(out1), None), S, PROF_REDUCE),
-        ("k_energy_windows", f"XYZ chain ({len(heis)} terms, {heis_groups} X-mask groups, "
-                             f"{heis_sweeps} window sweeps)",
+        ("k_pauli_group", f"XYZ chain ({len(heis)} terms, {heis_groups} X-mask groups)",
          lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(heis), len(heis),
-                      abi.Y_REFERENCE, C.byref(out1), None), heis_sweeps * S, PROF_REDUCE),
+                      abi.Y_REFERENCE, C.byref(out1), None), heis_groups * S, PROF_REDUCE),
         ("k_inner_partial", "inner product of two states",
          lambda: call("lq_inner_product", st.handle, other.handle, out2), 2 * S, PROF_REDUCE),
     ]

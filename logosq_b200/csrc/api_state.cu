@@ -232,27 +232,37 @@ __global__ void k_pauli_group(const A *__restrict__ v, int n, uint64_t xmask,
     for (int t = threadIdx.x; t < nt; t += blockDim.x) s_tc[t] = tc[t];
     __syncthreads();
     double acc[1] = {0.0};
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // The grid-stride loops take kU steps at a time with every load issued
+    // first (kU amplitudes, or kU pairs, in flight per thread); each thread
+    // still adds its steps in the same order.
+    constexpr int kU = 4;
     if (xmask == 0) {
         const uint64_t N = 1ull << n;
-        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
-             i += (uint64_t)gridDim.x * blockDim.x) {
-            const double2 a = load_amp(v, i);
+        auto add = [&](uint64_t i, double2 a) {
             double alpha = 0.0;
             for (int t = 0; t < nt; ++t) {
                 const double s = (__popcll(i & s_tc[t].z) & 1) ? -1.0 : 1.0;
                 alpha += s * s_tc[t].ca;
             }
             acc[0] += (a.x * a.x + a.y * a.y) * alpha;
+        };
+        uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+        for (; i + (kU - 1) * stride < N; i += kU * stride) {
+            double2 a[kU];
+#pragma unroll
+            for (int k = 0; k < kU; ++k) a[k] = load_amp(v, i + k * stride);
+#pragma unroll
+            for (int k = 0; k < kU; ++k) add(i + k * stride, a[k]);
         }
+        for (; i < N; i += stride) add(i, load_amp(v, i));
     } else {
         const int hb = 63 - __clzll(xmask);
         const uint64_t npairs = 1ull << (n - 1);
         const uint64_t lo_mask = (1ull << hb) - 1;
-        for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < npairs;
-             p += (uint64_t)gridDim.x * blockDim.x) {
-            const uint64_t i = ((p & ~lo_mask) << 1) | (p & lo_mask);
+        auto pair_index = [&](uint64_t p) { return ((p & ~lo_mask) << 1) | (p & lo_mask); };
+        auto add = [&](uint64_t i, double2 a, double2 b) {
             const uint64_t j = i ^ xmask;
-            const double2 a = load_amp(v, i), b = load_amp(v, j);
             // W_i = conj(a) b ; W_j = conj(W_i)
             const double wr = a.x * b.x + a.y * b.y;
             const double wi = a.x * b.y - a.y * b.x;
@@ -266,6 +276,22 @@ __global__ void k_pauli_group(const A *__restrict__ v, int n, uint64_t xmask,
                 be_j += sj * s_tc[t].cb;
             }
             acc[0] += wr * al_i + wi * be_i + wr * al_j - wi * be_j;
+        };
+        uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+        for (; p + (kU - 1) * stride < npairs; p += kU * stride) {
+            double2 a[kU], b[kU];
+#pragma unroll
+            for (int k = 0; k < kU; ++k) {
+                const uint64_t i = pair_index(p + k * stride);
+                a[k] = load_amp(v, i);
+                b[k] = load_amp(v, i ^ xmask);
+            }
+#pragma unroll
+            for (int k = 0; k < kU; ++k) add(pair_index(p + k * stride), a[k], b[k]);
+        }
+        for (; p < npairs; p += stride) {
+            const uint64_t i = pair_index(p);
+            add(i, load_amp(v, i), load_amp(v, i ^ xmask));
         }
     }
     block_sum<1>(acc, sh);
@@ -349,13 +375,6 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
         if (terms[t].ny != ny)
             return set_error(LQ_ERR_INVALID_ARG,
                              "Pauli term %d: ny=%d but xmask&zmask has %d bits", t, terms[t].ny, ny);
-    }
-    // Large states: one sweep per tile window instead of one per X mask.
-    if (!per_term) {
-        bool handled = false;
-        LQ_TRY(expectation_windows(const_cast<lq_state *>(s), terms, nterms, yconv, out,
-                                   &handled));
-        if (handled) return LQ_OK;
     }
     // Re(Y^ny z) selectors: Y = +i (reference convention) or -i (textbook).
     auto selectors = [&](int ny, double &a, double &b) {

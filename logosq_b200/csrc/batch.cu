@@ -321,169 +321,6 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
 
 static size_t batch_smem() { return (16u << kMaxT) + 2048; }
 
-// ---------------------------------------------------------------------------
-// Pauli-sum expectation of one state by tile windows (lq_expectation_pauli for
-// n >= kWindowMinQubits): the batch engine's energy windows applied to a state
-// in HBM.  A window is bits [0,4) U [h, h+8); a 2^12-amplitude tile holds every
-// pair (i, i ^ xmask) of the groups whose X bits lie in the window, so one
-// sweep of the state evaluates all of them (a 28-qubit XYZ chain: 4 sweeps
-// instead of one per X mask).
-// ---------------------------------------------------------------------------
-constexpr int kWindowMinQubits = 16;
-constexpr int kWindowCtasPerSm = 3;  // 67.6 KB of shared memory each
-
-// Each CTA sweeps tiles blockIdx.x, blockIdx.x + gridDim.x, ... of one window:
-// gathers the tile into shared memory (eight 16-byte loads in flight per
-// thread), adds the window's group contributions, and writes one FP64 partial.
-__global__ void __launch_bounds__(kBatchThreads, kWindowCtasPerSm)
-    k_energy_windows(const double2 *__restrict__ v, int h, uint64_t ntiles,
-                     const BGroup *__restrict__ groups, int ngroups,
-                     const BTerm *__restrict__ terms, double *__restrict__ partials) {
-    constexpr int T = kMaxT;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const uint32_t tile_a = smem_u32(base);
-    __shared__ double s_red[kBatchThreads / 32];
-    const int tid = threadIdx.x;
-    double acc = 0.0;
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const uint64_t c2 = t & ((1ull << (h - 4)) - 1);
-        const uint64_t c4 = t >> (h - 4);
-        const uint64_t tb = (c2 << 4) | (c4 << (h + T - 4));
-#pragma unroll
-        for (int k0 = 0; k0 < (1 << T) / kBatchThreads; k0 += 8) {
-            double2 r[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int l = tid + (k0 + k) * kBatchThreads;
-                r[k] = v[tb | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h)];
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int l = tid + (k0 + k) * kBatchThreads;
-                asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(tile_a +
-                                                                       ((uint32_t)swz(l) << 4)),
-                             "d"(r[k].x), "d"(r[k].y)
-                             : "memory");
-            }
-        }
-        __syncthreads();
-        acc += tile_energy(tile_a, T, h, tb, groups, 0, ngroups, terms, tid, kBatchThreads);
-        __syncthreads();  // before the next gather overwrites the tile
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((tid & 31) == 0) s_red[tid >> 5] = acc;
-    __syncthreads();
-    if (tid == 0) {
-        double e = 0.0;
-        for (int w = 0; w < kBatchThreads / 32; ++w) e += s_red[w];
-        partials[blockIdx.x] = e;
-    }
-}
-
-int expectation_windows(lq_state *s, const lq_pauli_term *terms, int nterms, int yconv,
-                        double *out, bool *handled) {
-    *handled = false;
-    const int n = s->n, m = kMaxT - 4;
-    if (s->dtype != LQ_C128 || n < kWindowMinQubits || nterms < 1) return LQ_OK;
-    std::map<uint64_t, std::vector<int>> byx;
-    for (int t = 0; t < nterms; ++t) byx[terms[t].xmask].push_back(t);
-    // Each group with X bits above bit 3 needs h in [max(4, hb - m + 1), min(lb, n - m)];
-    // groups without such bits fit every window.
-    struct Span {
-        int lo, hi;
-        uint64_t x;
-    };
-    std::vector<Span> spans;
-    std::vector<uint64_t> anywhere;
-    for (auto &kv : byx) {
-        const uint64_t hx = kv.first & ~0xFull;
-        if (!hx) {
-            anywhere.push_back(kv.first);
-            continue;
-        }
-        const int lb = __builtin_ctzll(hx), hb = 63 - __builtin_clzll(hx);
-        const int lo = std::max(4, hb - m + 1), hi = std::min(lb, n - m);
-        if (lo > hi) return LQ_OK;  // X bits wider than one window: per-group sweeps
-        spans.push_back({lo, hi, kv.first});
-    }
-    // Fewest windows: greedy stabbing at the smallest open right end.
-    std::sort(spans.begin(), spans.end(), [](const Span &a, const Span &b) {
-        return a.hi != b.hi ? a.hi < b.hi : a.x < b.x;
-    });
-    std::vector<std::pair<int, std::vector<uint64_t>>> wins;
-    std::vector<char> done(spans.size(), 0);
-    for (size_t i = 0; i < spans.size(); ++i) {
-        if (done[i]) continue;
-        const int h = spans[i].hi;
-        std::vector<uint64_t> xs;
-        for (size_t j = i; j < spans.size(); ++j)
-            if (!done[j] && spans[j].lo <= h) {
-                done[j] = 1;
-                xs.push_back(spans[j].x);
-            }
-        wins.push_back({h, xs});
-    }
-    if (wins.empty()) wins.push_back({4, {}});
-    for (uint64_t x : anywhere) wins[0].second.push_back(x);
-
-    int dev = 0, sms = 0;
-    LQ_CUDA_TRY(cudaGetDevice(&dev));
-    LQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint64_t ntiles = 1ull << (n - kMaxT);
-    const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kWindowCtasPerSm * sms);
-    const size_t nwin = wins.size();
-    if (nwin * grid > (size_t)kRedBlocks * 2 * kMaxTermsPerPass - 8) return LQ_OK;
-
-    // Y^ny phase as selectors of Re(i^k (x + i y)) (see expectation_impl).
-    std::vector<BGroup> groups;
-    std::vector<BTerm> bterms;
-    std::vector<int> wbeg, wcnt;
-    for (auto &w : wins) {
-        wbeg.push_back((int)groups.size());
-        for (uint64_t x : w.second) {
-            groups.push_back(BGroup{x, (int)bterms.size(), (int)byx[x].size()});
-            for (int t : byx[x]) {
-                int k = terms[t].ny & 3;
-                if (yconv == LQ_Y_TEXTBOOK) k = (4 - k) & 3;
-                const double a = k == 0 ? 1.0 : k == 2 ? -1.0 : 0.0;
-                const double b = k == 1 ? -1.0 : k == 3 ? 1.0 : 0.0;
-                bterms.push_back(BTerm{terms[t].zmask, terms[t].coefficient * a,
-                                       terms[t].coefficient * b});
-            }
-        }
-        wcnt.push_back((int)groups.size() - wbeg.back());
-    }
-    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t tb_bytes = bterms.size() * sizeof(BTerm), gb_bytes = groups.size() * sizeof(BGroup);
-    LQ_TRY(ensure_prog(s, al(tb_bytes) + al(gb_bytes) + 256));
-    BTerm *d_terms = (BTerm *)s->d_prog;
-    BGroup *d_groups = (BGroup *)((char *)s->d_prog + al(tb_bytes));
-    LQ_CUDA_TRY(cudaMemcpyAsync(d_terms, bterms.data(), tb_bytes, cudaMemcpyHostToDevice,
-                                s->stream));
-    LQ_CUDA_TRY(cudaMemcpyAsync(d_groups, groups.data(), gb_bytes, cudaMemcpyHostToDevice,
-                                s->stream));
-    LQ_CUDA_TRY(cudaFuncSetAttribute(k_energy_windows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)batch_smem()));
-    prof_begin(s->stream, kProfReduce);
-    for (size_t w = 0; w < nwin; ++w)
-        k_energy_windows<<<grid, kBatchThreads, batch_smem(), s->stream>>>(
-            (const double2 *)s->d, wins[w].first, ntiles, d_groups + wbeg[w], wcnt[w], d_terms,
-            s->d_red + w * grid);
-    prof_end(s->stream, kProfReduce);
-    LQ_CUDA_TRY(cudaGetLastError());
-    std::vector<double> part(nwin * grid);
-    LQ_CUDA_TRY(cudaMemcpyAsync(part.data(), s->d_red, part.size() * sizeof(double),
-                                cudaMemcpyDeviceToHost, s->stream));
-    LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    double sum = 0.0;  // fixed order: window by window, CTA by CTA
-    for (double x : part) sum += x;
-    *out = sum;
-    *handled = true;
-    return LQ_OK;
-}
-
 // 2x2 matrix (m00, m01, m10, m11 as re/im pairs) of an uncontrolled
 // single-qubit op and the index bit it acts on; false for any other op.
 static bool single_bit_matrix(const GateOp &g, int &bit, double m[8]) {

@@ -102,11 +102,6 @@ int gate_class(int kind);
 int normalize_impl(lq_state *s);
 int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, int yconv,
                      double *out, double *per_term);
-// batch.cu: the same sum by tile windows, one sweep per window (complex128,
-// n >= 16, every X-mask group within one window).  Sets *handled = false and
-// does nothing otherwise.
-int expectation_windows(lq_state *s, const lq_pauli_term *terms, int nterms, int yconv,
-                        double *out, bool *handled);
 
 // profile.cu: optional CUDA-event timing of launches, by kernel class.
 enum ProfClass { kProfFused = 0, kProfGate = 1, kProfReduce = 2, kProfBatch = 3, kProfTc = 4,

@@ -1,9 +1,9 @@
-"""GPU: Pauli-sum expectation of large states by tile windows (complex128,
-n >= 16): every X-mask group whose X bits above bit 3 fit eight consecutive
-bits is evaluated from 2^12-amplitude tiles, one sweep of the state per window.
-Checked against the oracle (PauliObservable::expectation,
-src/optimization/observable.rs:95-147, 228-232) and against the per-group
-sweeps (the path taken when per-term values are requested), 1e-12 relative."""
+"""GPU: Pauli-sum expectation of 16- to 22-qubit states (complex128) against the
+oracle (PauliObservable::expectation, src/optimization/observable.rs:95-147,
+228-232) and against the per-term evaluation (one sweep per term instead of
+one per X-mask group), 1e-12 relative: X masks local to a few bits, only in
+bits 0-3, at the top bits, across bit 3/4 and spanning the whole index, Z-only
+terms, both Y conventions, XYZ chains, and run-to-run determinism."""
 import ctypes as C
 
 import numpy as np
@@ -36,7 +36,7 @@ def pack(specs):
     return terms
 
 
-def windowed_terms(n, count, seed):
+def local_x_terms(n, count, seed):
     """Random terms whose X bits above bit 3 lie in one random 8-bit range,
     plus Z-only terms and terms with X bits only in bits 0-3."""
     rng = workloads.SplitMix64(seed)
@@ -66,16 +66,16 @@ def check(n, terms, seed):
             want = oracle.expectation(v, terms, yc)
             got, _ = expect(st, terms, yc)
             assert abs(got - want) <= TOL * max(1.0, abs(want)), (n, yc, got, want)
-            sweeps, per = expect(st, terms, yc, per_term=True)
-            assert abs(got - sweeps) <= TOL * max(1.0, abs(want))
+            by_term, per = expect(st, terms, yc, per_term=True)
+            assert abs(got - by_term) <= TOL * max(1.0, abs(want))
             assert abs(per.sum() - want) <= TOL * max(1.0, abs(want))
     finally:
         st.close()
 
 
 @pytest.mark.parametrize("n", [16, 18, 20])
-def test_random_windowed_sums_vs_oracle(n):
-    check(n, windowed_terms(n, 48, seed=n), seed=100 + n)
+def test_random_sums_vs_oracle(n):
+    check(n, local_x_terms(n, 48, seed=n), seed=100 + n)
 
 
 def test_top_bits_and_bit3_straddle():
@@ -87,7 +87,7 @@ def test_top_bits_and_bit3_straddle():
     check(n, pack(specs), seed=7)
 
 
-def test_wide_x_mask_falls_back_to_group_sweeps():
+def test_wide_x_masks():
     n = 18
     specs = [(0.5, (1 << 4) | (1 << 17), 0), (0.25, (1 << 6) | (1 << 7), 1 << 6),
              (-0.8, 0, 0b101)]
@@ -102,9 +102,9 @@ def test_xyz_chain_vs_oracle(n):
     check(n, terms, seed=200 + n)
 
 
-def test_windowed_result_is_deterministic():
+def test_result_is_deterministic():
     n = 20
-    terms = windowed_terms(n, 32, seed=3)
+    terms = local_x_terms(n, 32, seed=3)
     v = random_state(n, 5)
     st = State.zero_state(n)
     try:
