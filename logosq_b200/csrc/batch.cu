@@ -46,6 +46,8 @@ struct BEWin {  // energy window: groups whose X bits lie inside [0,4) U [h, h+T
 struct BGroup {
     uint64_t xmask;
     int32_t term_begin, nterms;
+    uint32_t lx;  // X mask in tile-local bits (bits 0-3 stay, bit b >= h maps to 4 + b - h)
+    int32_t pad;
 };
 
 struct BTerm {
@@ -130,12 +132,7 @@ __device__ double tile_energy(uint32_t tile_a, int T, int h, uint64_t tile_base,
     const int m = T - 4;
     for (int g = g0; g < g0 + ng; ++g) {
         const BGroup gr = groups[g];
-        // local X mask
-        uint32_t lx = 0;
-        for (int b = 0; b < 64; ++b) {
-            if (!((gr.xmask >> b) & 1)) continue;
-            lx |= 1u << (b < 4 ? b : 4 + (b - h));
-        }
+        const uint32_t lx = gr.lx;
         const BTerm *tp = terms + gr.term_begin;
         if (lx == 0) {
             for (int l = tid; l < (1 << T); l += nthr) {
@@ -740,7 +737,10 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
             for (auto &w : win) {
                 BEWin ew{w.first, (int)groups.size(), (int)w.second.size(), 0};
                 for (uint64_t x : w.second) {
-                    BGroup g{x, (int)bterms.size(), (int)byx[x].size()};
+                    uint32_t lx = 0;  // the window holds every X bit (chosen above)
+                    for (int bt = 0; bt < n; ++bt)
+                        if ((x >> bt) & 1) lx |= 1u << (bt < 4 ? bt : 4 + (bt - w.first));
+                    BGroup g{x, (int)bterms.size(), (int)byx[x].size(), lx, 0};
                     for (int t : byx[x]) {
                         const lq_pauli_term &pt = b->terms[i][t];
                         int k = pt.ny & 3;  // reference convention: Y = +i
