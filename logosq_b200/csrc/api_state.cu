@@ -262,20 +262,19 @@ __global__ void k_pauli_group(const A *__restrict__ v, int n, uint64_t xmask,
         const uint64_t lo_mask = (1ull << hb) - 1;
         auto pair_index = [&](uint64_t p) { return ((p & ~lo_mask) << 1) | (p & lo_mask); };
         auto add = [&](uint64_t i, double2 a, double2 b) {
-            const uint64_t j = i ^ xmask;
-            // W_i = conj(a) b ; W_j = conj(W_i)
+            // W_i = conj(a) b ; W_j = conj(W_i), j = i ^ xmask.  The j-side sums
+            // follow from the i side: a term's Z sign at j is its sign at i times
+            // (-1)^ny, and ca = 0 for odd ny, cb = 0 for even ny, so
+            // al_j = al_i and be_j = -be_i.
             const double wr = a.x * b.x + a.y * b.y;
             const double wi = a.x * b.y - a.y * b.x;
-            double al_i = 0.0, be_i = 0.0, al_j = 0.0, be_j = 0.0;
+            double al_i = 0.0, be_i = 0.0;
             for (int t = 0; t < nt; ++t) {
                 const double si = (__popcll(i & s_tc[t].z) & 1) ? -1.0 : 1.0;
-                const double sj = (__popcll(j & s_tc[t].z) & 1) ? -1.0 : 1.0;
                 al_i += si * s_tc[t].ca;
                 be_i += si * s_tc[t].cb;
-                al_j += sj * s_tc[t].ca;
-                be_j += sj * s_tc[t].cb;
             }
-            acc[0] += wr * al_i + wi * be_i + wr * al_j - wi * be_j;
+            acc[0] += 2.0 * (wr * al_i + wi * be_i);
         };
         uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
         for (; p + (kU - 1) * stride < npairs; p += kU * stride) {

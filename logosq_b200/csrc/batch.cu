@@ -152,7 +152,6 @@ __device__ double tile_energy(uint32_t tile_a, int T, int h, uint64_t tile_base,
                 const int l = (int)insert_zero_u((uint64_t)p, hb);
                 const int j = l ^ (int)lx;
                 const uint64_t gi = tile_base | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h);
-                const uint64_t gj = gi ^ gr.xmask;
                 double2 a, b;
                 asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
                              : "=d"(a.x), "=d"(a.y)
@@ -162,15 +161,16 @@ __device__ double tile_energy(uint32_t tile_a, int T, int h, uint64_t tile_base,
                              : "r"(tile_a + ((uint32_t)swz(j) << 4)));
                 const double wr = a.x * b.x + a.y * b.y;
                 const double wi = a.x * b.y - a.y * b.x;
-                double ai = 0.0, bi = 0.0, aj = 0.0, bj = 0.0;
+                // The j-side sums follow from the i side: a term's Z sign at j is
+                // its sign at i times (-1)^ny, and ca = 0 for odd ny, cb = 0 for
+                // even ny, so aj = ai and bj = -bi.
+                double ai = 0.0, bi = 0.0;
                 for (int t = 0; t < gr.nterms; ++t) {
-                    const bool si = __popcll(gi & tp[t].z) & 1, sj = __popcll(gj & tp[t].z) & 1;
+                    const bool si = __popcll(gi & tp[t].z) & 1;
                     ai += si ? -tp[t].ca : tp[t].ca;
                     bi += si ? -tp[t].cb : tp[t].cb;
-                    aj += sj ? -tp[t].ca : tp[t].ca;
-                    bj += sj ? -tp[t].cb : tp[t].cb;
                 }
-                acc += wr * ai + wi * bi + wr * aj - wi * bj;
+                acc += 2.0 * (wr * ai + wi * bi);
             }
         }
         (void)m;
