@@ -297,6 +297,60 @@ __global__ void k_pauli_group(const A *__restrict__ v, int n, uint64_t xmask,
     if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
 }
 
+// Terms without X bits (one group, X mask 0), for states of 12 or more qubits,
+// launched with 256 threads.  A block takes 4096-amplitude chunks; thread tid
+// handles the 16 indices i = chunk | k << 8 | tid, k = 0..15.  A term's sign
+// (-1)^popcount(i & z) is the sign of the bits the thread keeps fixed (chunk
+// and tid) times (-1)^popcount(k & p), p = bits 8-11 of z.  The terms arrive
+// sorted by p (pbeg[p] .. pbeg[p+1]), so each thread folds all of them into 16
+// coefficients C[p], and one 16-point Walsh-Hadamard transform of C gives the
+// sum of signed coefficients for all 16 k: a few operations per amplitude
+// instead of a popcount and a select per term per amplitude.
+template <class A>
+__global__ void __launch_bounds__(256, 2)
+    k_pauli_zfold(const A *__restrict__ v, int n, const TermCoef *__restrict__ tc, int nt,
+                  const int *__restrict__ pbeg, double *partials) {
+    extern __shared__ TermCoef s_tc[];
+    __shared__ double sh[32];
+    __shared__ int s_pbeg[17];
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) s_tc[t] = tc[t];
+    if (threadIdx.x < 17) s_pbeg[threadIdx.x] = pbeg[threadIdx.x];
+    __syncthreads();
+    double acc[1] = {0.0};
+    const uint64_t nchunks = 1ull << (n - 12);
+    for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const uint64_t fixed = (c << 12) | (uint64_t)threadIdx.x;
+        double pr[16];  // |a|^2 of the 16 amplitudes
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const double2 a = load_amp(v, fixed | ((uint64_t)k << 8));
+            pr[k] = a.x * a.x + a.y * a.y;
+        }
+        double C[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            double cq = 0.0;
+            for (int t = s_pbeg[q]; t < s_pbeg[q + 1]; ++t)
+                cq += (__popcll(fixed & s_tc[t].z) & 1) ? -s_tc[t].ca : s_tc[t].ca;
+            C[q] = cq;
+        }
+#pragma unroll
+        for (int hs = 1; hs < 16; hs <<= 1) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                if (q & hs) continue;
+                const double x = C[q], y = C[q | hs];
+                C[q] = x + y;
+                C[q | hs] = x - y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc[0] += pr[k] * C[k];
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -403,6 +457,24 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
     const uint64_t N = 1ull << n;
     const int th = 256;
     const int g = red_grid(std::max<uint64_t>(N / 2, 1), th);
+    // The X-mask-0 group of a state with 12 or more qubits runs the folded form
+    // (k_pauli_zfold): its terms sorted by bits 8-11 of the Z mask.
+    int zfold = -1;
+    int pbeg[17] = {0};
+    if (!per_term && n >= 12) {
+        for (size_t gi = 0; gi < groups.size(); ++gi)
+            if (groups[gi].first == 0) zfold = (int)gi;
+    }
+    if (zfold >= 0) {
+        auto pat = [&](int t) { return (int)((terms[t].zmask >> 8) & 15); };
+        std::vector<int> &ts = groups[zfold].second;
+        std::stable_sort(ts.begin(), ts.end(), [&](int x, int y) { return pat(x) < pat(y); });
+        for (int q = 0; q <= 16; ++q) {
+            int k = 0;
+            while (k < (int)ts.size() && pat(ts[k]) < q) ++k;
+            pbeg[q] = k;
+        }
+    }
     // Host-side packed coefficients, uploaded once per call.
     std::vector<TermCoef> tc(nterms);
     std::vector<int> offs;
@@ -421,22 +493,35 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
     lq_state *ms = const_cast<lq_state *>(s);
     const size_t coef_bytes = packed.size() * sizeof(TermCoef);
     const size_t res_bytes = groups.size() * sizeof(double);
-    LQ_TRY(ensure_prog(ms, coef_bytes + res_bytes + 256));
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    LQ_TRY(ensure_prog(ms, al(coef_bytes) + al(res_bytes) + sizeof(pbeg) + 256));
     TermCoef *d_tc = (TermCoef *)ms->d_prog;
-    double *d_res = (double *)((char *)ms->d_prog + ((coef_bytes + 255) / 256) * 256);
+    double *d_res = (double *)((char *)ms->d_prog + al(coef_bytes));
+    int *d_pbeg = (int *)((char *)ms->d_prog + al(coef_bytes) + al(res_bytes));
     if (!packed.empty())
         LQ_CUDA_TRY(cudaMemcpyAsync(d_tc, packed.data(), coef_bytes, cudaMemcpyHostToDevice,
+                                    s->stream));
+    if (zfold >= 0)
+        LQ_CUDA_TRY(cudaMemcpyAsync(d_pbeg, pbeg, sizeof(pbeg), cudaMemcpyHostToDevice,
                                     s->stream));
     prof_begin(s->stream, kProfReduce);
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const int nt = (int)groups[gi].second.size();
         const size_t shm = nt * sizeof(TermCoef);
-        if (s->dtype == LQ_C128)
+        if ((int)gi == zfold) {
+            if (s->dtype == LQ_C128)
+                k_pauli_zfold<<<g, th, shm, s->stream>>>((const double2 *)s->d, n,
+                                                         d_tc + offs[gi], nt, d_pbeg, s->d_red);
+            else
+                k_pauli_zfold<<<g, th, shm, s->stream>>>((const float2 *)s->d, n,
+                                                         d_tc + offs[gi], nt, d_pbeg, s->d_red);
+        } else if (s->dtype == LQ_C128) {
             k_pauli_group<<<g, th, shm, s->stream>>>((const double2 *)s->d, n, groups[gi].first,
                                                      d_tc + offs[gi], nt, s->d_red);
-        else
+        } else {
             k_pauli_group<<<g, th, shm, s->stream>>>((const float2 *)s->d, n, groups[gi].first,
                                                      d_tc + offs[gi], nt, s->d_red);
+        }
         k_final_sum<1><<<1, 256, 0, s->stream>>>(s->d_red, g, d_res + gi);
     }
     prof_end(s->stream, kProfReduce);
