@@ -467,10 +467,10 @@ def run_kernels(args):
          lambda: call("lq_apply_block", st.handle, 4, q4, abi.f64_ptr(m4)), 2 * S, PROF_FUSED),
         ("k_norm_partial", "norm_sqr", lambda: call("lq_norm_sqr", st.handle, C.byref(out1)),
          S, PROF_REDUCE),
-        ("k_pauli_group", "one Z-string term",
+        ("k_pauli_zfold", "one Z-string term",
          lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(zstring), 1,
                       abi.Y_REFERENCE, C.byref(out1), None), S, PROF_REDUCE),
-        ("k_pauli_group", f"XYZ chain ({len(heis)} terms, {heis_groups} X-mask groups)",
+        ("k_pauli_group + k_pauli_zfold", f"XYZ chain ({len(heis)} terms, {heis_groups} X-mask groups)",
          lambda: call("lq_expectation_pauli", st.handle, abi.term_ptr(heis), len(heis),
                       abi.Y_REFERENCE, C.byref(out1), None), heis_groups * S, PROF_REDUCE),
         ("k_inner_partial", "inner product of two states",

@@ -88,3 +88,44 @@ def test_pair_formula_on_xyz_chain():
     v = workloads.gaussian_state(n, 4)
     want = oracle.expectation(v, terms, abi.Y_REFERENCE)
     assert abs(pair_formula(v, terms, False) - want) < 1e-12 * max(1.0, abs(want))
+
+
+def zfold_formula(v, terms):
+    """The folded form of the X-mask-0 group (k_pauli_zfold), vectorised over the
+    256 threads: per 4096-amplitude chunk and thread, the terms' signs at the
+    bits the thread keeps fixed are folded into 16 coefficients by bits 8-11 of
+    z, and a Walsh-Hadamard transform gives the signed sum for each k."""
+    n = int(np.log2(len(v)))
+    pr = np.abs(v) ** 2
+    z = terms["zmask"].astype(np.int64)
+    ca = terms["coefficient"].astype(np.float64)  # X mask 0: the real selector is 1
+    pat = (z >> 8) & 15
+    tid = np.arange(256, dtype=np.int64)
+    total = 0.0
+    for c in range(1 << (n - 12)):
+        fixed = (c << 12) | tid
+        C = np.zeros((16, 256))
+        for t in range(len(z)):
+            par = np.array([bin(int(f) & int(z[t])).count("1") & 1 for f in fixed])
+            C[pat[t]] += np.where(par == 1, -ca[t], ca[t])
+        hs = 1
+        while hs < 16:
+            for q in range(16):
+                if not q & hs:
+                    C[q], C[q | hs] = C[q] + C[q | hs], C[q] - C[q | hs]
+            hs <<= 1
+        for k in range(16):
+            total += float(np.sum(pr[fixed | (k << 8)] * C[k]))
+    return total
+
+
+def test_zfold_formula_matches_oracle():
+    n = 13
+    rng = workloads.SplitMix64(17)
+    terms = np.zeros(30, dtype=abi.TERM_DTYPE)
+    for t in range(30):
+        terms[t]["coefficient"] = rng.uniform(-1, 1)
+        terms[t]["zmask"] = rng.randint(0, (1 << n) - 1)
+    v = workloads.gaussian_state(n, 8)
+    want = oracle.expectation(v, terms, abi.Y_REFERENCE)
+    assert abs(zfold_formula(v, terms) - want) < 1e-12 * max(1.0, abs(want))
