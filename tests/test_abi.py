@@ -71,3 +71,12 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(_lib.LogosQError):
         _lib.lib()
+
+
+def test_integration_binding_covers_header():
+    """The Rust binding written out for a LogosQ maintainer binds every entry
+    point the header declares."""
+    text = (ROOT / "INTEGRATION.md").read_text()
+    bound = set(re.findall(r"pub fn (lq_\w+)\(", text))
+    missing = [n for n in declared_functions() if n not in bound]
+    assert not missing, missing
