@@ -79,3 +79,41 @@ def test_pair_fold_emits_4x4_ops_and_matches_oracle(kind):
     assert (m2["k0"] < m2["k1"]).all()
     v = random_state(n, 4)
     assert np.abs(fe.run(n, g, v) - oracle.apply_circuit(v.copy(), g)).max() < 1e-12
+
+
+def _with_width(width, fn):
+    import ctypes as C
+    from logosq_b200._lib import call
+    w0 = C.c_int()
+    call("lq_get_fusion_width", C.byref(w0))
+    call("lq_set_fusion_width", width)
+    try:
+        return fn()
+    finally:
+        call("lq_set_fusion_width", w0.value)
+
+
+@pytest.mark.parametrize("width", [5, 6, 8, 10, 11, 12])
+@pytest.mark.parametrize("n,seed", [(9, 21), (13, 22), (16, 23)])
+def test_emulated_random_circuits_at_every_width(width, n, seed):
+    """The planner and encoder at every tile width the engine accepts (the
+    autotuner picks 10, 11 or 12; lq_set_fusion_width allows 5..12), on random
+    circuits of every gate kind."""
+    g = random_circuit(n, 30 + 2 * n, seed)
+    v = random_state(n, seed)
+
+    def check():
+        T = fe.dump(n, g)[0]
+        assert T == min(width, n)
+        assert np.abs(fe.run(n, g, v) - oracle.apply_circuit(v.copy(), g)).max() < 1e-12
+
+    _with_width(width, check)
+
+
+@pytest.mark.parametrize("width", [10, 11, 12])
+def test_emulated_brickwork_at_autotuned_widths(width):
+    n = 16
+    g = workloads.brickwork_u3(n, 8, seed=5)
+    v = random_state(n, 9)
+    _with_width(width, lambda: np.testing.assert_allclose(
+        fe.run(n, g, v), oracle.apply_circuit(v.copy(), g), rtol=0, atol=1e-12))
