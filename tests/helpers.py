@@ -19,10 +19,12 @@ def known_answers():
     return json.loads((GOLDEN / "known_answers.json").read_text())
 
 
-def perm_matrix(pairs, dim):
+def perm_matrix(entries, dim):
+    """dim x dim matrix from [row, col] entries equal to 1, or [row, col, value]
+    entries with a real value."""
     m = np.zeros((dim, dim), dtype=np.complex128)
-    for r, c in pairs:
-        m[r, c] = 1.0
+    for e in entries:
+        m[e[0], e[1]] = e[2] if len(e) > 2 else 1.0
     return m
 
 
