@@ -17,8 +17,8 @@ from .circuits import Circuit, Operation
 from .optimization import (Pauli, PauliTerm, PauliObservable, Observable, Ansatz,
                            HardwareEfficientAnsatz, RealAmplitudesAnsatz, EfficientSU2Ansatz,
                            ParameterizedCircuit, EntanglingGate, EntanglingPattern,
-                           ParameterShift, FiniteDifference, GradientDescent, Adam, VQE,
-                           QuantumNaturalGradient)
+                           ParameterShift, FiniteDifference, GradientDescent, Adam, LBFGSB,
+                           OptimizerResult, VQE, QuantumNaturalGradient)
 from .algorithms import qft, rqc, xyz_heisenberg
 from .qml import VariationalQuantumCircuit, VQCType
 
@@ -27,7 +27,8 @@ __all__ = [
     "Operation", "Pauli", "PauliTerm", "PauliObservable", "Observable", "Ansatz",
     "HardwareEfficientAnsatz", "RealAmplitudesAnsatz", "EfficientSU2Ansatz",
     "ParameterizedCircuit", "EntanglingGate", "EntanglingPattern", "ParameterShift",
-    "FiniteDifference", "GradientDescent", "Adam", "VQE", "QuantumNaturalGradient",
+    "FiniteDifference", "GradientDescent", "Adam", "LBFGSB", "OptimizerResult", "VQE",
+    "QuantumNaturalGradient",
     "qft", "rqc", "xyz_heisenberg",
     "VariationalQuantumCircuit", "VQCType",
 ]

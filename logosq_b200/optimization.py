@@ -482,6 +482,11 @@ class GradientDescent:
         self.learning_rate, self.max_iterations = learning_rate, max_iterations
         self.tolerance, self.verbose = tolerance, verbose
 
+    def with_tolerance(self, tolerance) -> "GradientDescent":
+        """GradientDescent::with_tolerance (src/optimization/optimizer.rs:50-53)."""
+        self.tolerance = tolerance
+        return self
+
     def minimize(self, f, grad_f, initial_params):
         params = np.array(initial_params, dtype=np.float64)
         hist, converged = [], False
@@ -511,6 +516,11 @@ class Adam:
         self.learning_rate, self.max_iterations = learning_rate, max_iterations
         self.beta1, self.beta2, self.epsilon = 0.9, 0.999, 1e-8
         self.tolerance, self.verbose = tolerance, verbose
+
+    def with_tolerance(self, tolerance) -> "Adam":
+        """Adam::with_tolerance (src/optimization/optimizer.rs:132-135)."""
+        self.tolerance = tolerance
+        return self
 
     def minimize(self, f, grad_f, initial_params):
         params = np.array(initial_params, dtype=np.float64)
@@ -549,6 +559,15 @@ class Adam:
         if math.sqrt(float(np.sum(fg * fg))) < self.tolerance:
             converged = True
         return OptimizerResult(params, opt, len(hist), hist, converged)
+
+
+class LBFGSB:
+    """LBFGSB (src/optimization/optimizer.rs:227-241): the reference declares
+    the optimizer's settings (iterations, tolerance 1e-6, memory 10) and no
+    minimisation routine; the mirror keeps the same interface."""
+
+    def __init__(self, max_iterations):
+        self.max_iterations, self.tolerance, self.m = max_iterations, 1e-6, 10
 
 
 class VQEResult:
