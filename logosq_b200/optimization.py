@@ -114,14 +114,23 @@ class PauliObservable(Observable):
             self._packed = pack_terms(self.terms, self.num_qubits)
         return self._packed
 
+    @staticmethod
+    def _check_qubit(q, num_qubits):
+        # The reference asserts "Qubit index out of bounds" (observable.rs:177, 193-194, 210).
+        if not 0 <= q < num_qubits:
+            raise LogosQError(abi.LQ_ERR_QUBIT_INDEX, "Qubit index out of bounds")
+
     @classmethod
     def single_z(cls, num_qubits, target_qubit):
+        cls._check_qubit(target_qubit, num_qubits)
         p = [Pauli.I] * num_qubits
         p[target_qubit] = Pauli.Z
         return cls.from_terms(num_qubits, [PauliTerm(1.0, p)])
 
     @classmethod
     def zz_interaction(cls, num_qubits, qubit1, qubit2, coefficient):
+        cls._check_qubit(qubit1, num_qubits)
+        cls._check_qubit(qubit2, num_qubits)
         p = [Pauli.I] * num_qubits
         p[qubit1] = Pauli.Z
         p[qubit2] = Pauli.Z
@@ -131,11 +140,13 @@ class PauliObservable(Observable):
     def ising_hamiltonian(cls, num_qubits, j_couplings, h_fields):
         o = cls(num_qubits)
         for i, j in enumerate(j_couplings):
+            cls._check_qubit(i + 1, num_qubits)
             p = [Pauli.I] * num_qubits
             p[i] = Pauli.Z
             p[i + 1] = Pauli.Z
             o.add_term(PauliTerm(j, p))
         for i, hf in enumerate(h_fields):
+            cls._check_qubit(i, num_qubits)
             p = [Pauli.I] * num_qubits
             p[i] = Pauli.Z
             o.add_term(PauliTerm(hf, p))

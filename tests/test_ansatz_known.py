@@ -73,3 +73,25 @@ def test_wrong_parameter_count():
     with pytest.raises(LogosQError, match="Parameter count mismatch") as ei:
         a.build_circuit([0.1, 0.2])
     assert ei.value.code == abi.LQ_ERR_PARAM_COUNT
+
+
+def test_observable_wrong_qubit_index():
+    """tests/test_optimization.rs:288-292: single_z on a qubit the system lacks."""
+    from logosq_b200 import PauliObservable
+    with pytest.raises(LogosQError, match="Qubit index out of bounds") as ei:
+        PauliObservable.single_z(2, 3)
+    assert ei.value.code == abi.LQ_ERR_QUBIT_INDEX
+
+
+def test_zero_depth_and_single_qubit_parameter_counts():
+    """tests/test_optimization.rs:305-334 (parameter counts)."""
+    assert HardwareEfficientAnsatz(2, 0, EntanglingGate.CNOT,
+                                   EntanglingPattern.Linear).num_parameters() == 2
+    assert RealAmplitudesAnsatz(1, 1).num_parameters() == 2
+
+
+def test_ansatz_scaling():
+    """tests/test_optimization.rs:351-367"""
+    for n in range(1, 5):
+        a = HardwareEfficientAnsatz(n, 1, EntanglingGate.CNOT, EntanglingPattern.Linear)
+        assert a.build_circuit([0.1] * a.num_parameters()).num_qubits() == n
