@@ -95,3 +95,13 @@ def test_ansatz_scaling():
     for n in range(1, 5):
         a = HardwareEfficientAnsatz(n, 1, EntanglingGate.CNOT, EntanglingPattern.Linear)
         assert a.build_circuit([0.1] * a.num_parameters()).num_qubits() == n
+
+
+def test_qft_circuit_creation():
+    """tests/test_qft.rs:12-28 and 30-42: names and non-empty operation lists."""
+    from logosq_b200 import qft
+    c = qft.create_circuit(3)
+    assert c.num_qubits() == 3 and "Quantum Fourier Transform" in c.name()
+    assert len(c.operations()) > 0
+    ci = qft.create_inverse_circuit(3)
+    assert ci.num_qubits() == 3 and "Inverse" in ci.name() and len(ci.operations()) > 0
