@@ -21,16 +21,25 @@ class Operation:
     """One operation (src/circuits/mod.rs:29-33): a descriptor, or a full dense
     matrix (MatrixGate) which runs as its own dense kernel."""
 
-    __slots__ = ("desc", "dense", "qubits", "name")
+    __slots__ = ("desc", "dense", "_qubits", "_name")
 
     def __init__(self, desc, qubits, name, dense=None):
         self.desc = desc
         self.dense = dense
-        self.qubits = list(qubits)
-        self.name = name
+        self._qubits = list(qubits)
+        self._name = name
+
+    def qubits(self):
+        """Operation::qubits (src/circuits/mod.rs:51-53)."""
+        return self._qubits
+
+    def name(self):
+        """Operation::name (src/circuits/mod.rs:56-58)."""
+        return self._name
 
     def __repr__(self):
-        return f"{self.name}(qubits: {self.qubits})"
+        # Debug for Operation (src/circuits/mod.rs:61-65)
+        return f"{self._name}(qubits: {self._qubits})"
 
 
 def _expand_single(matrix, target, n):
@@ -202,10 +211,17 @@ class Circuit:
         self._packed = None
         return self
 
+    def clone(self) -> "Circuit":
+        """Circuit::clone: a copy whose operation list is independent."""
+        c = Circuit(self._n)
+        c._ops = list(self._ops)
+        c._name = self._name
+        return c
+
     def reversed(self) -> "Circuit":
         c = Circuit(self._n)
         for op in reversed(self._ops):
-            c._ops.append(Operation(op.desc, op.qubits, f"reversed_{op.name}", op.dense))
+            c._ops.append(Operation(op.desc, op.qubits(), f"reversed_{op.name()}", op.dense))
         if self._name:
             c._name = f"{self._name}_reversed"
         return c
@@ -310,4 +326,7 @@ class Circuit:
         return out
 
     def __repr__(self):
-        return f"Circuit(n={self._n}, ops={len(self._ops)}, name={self._name!r})"
+        # Debug for Circuit (src/circuits/mod.rs:597-608)
+        lines = [f"Circuit: {self._name or 'Unnamed Circuit'} ({self._n} qubits)"]
+        lines += [f"{i}: {op!r}" for i, op in enumerate(self._ops)]
+        return "\n".join(lines) + "\n"

@@ -348,3 +348,25 @@ def swap_matrix():
 
 def cz_matrix():
     return np.diag([1, 1, 1, -1]).astype(np.complex128)
+
+
+def toffoli_matrix():
+    m = np.eye(8, dtype=np.complex128)
+    m[[6, 7]] = m[[7, 6]]
+    return m
+
+
+# ---- gates::matrix constructors (src/gates/matrix.rs:14-261): MatrixGate ----
+def x_gate(): return MatrixGate(x_matrix())
+def y_gate(): return MatrixGate(y_matrix())
+def z_gate(): return MatrixGate(z_matrix())
+def h_gate(): return MatrixGate(h_matrix())
+def s_gate(): return MatrixGate(s_matrix())
+def t_gate(): return MatrixGate(t_matrix())
+def rx_gate(theta): return MatrixGate(rx_matrix(theta))
+def ry_gate(theta): return MatrixGate(ry_matrix(theta))
+def rz_gate(theta): return MatrixGate(rz_matrix(theta))
+def cnot_gate(): return MatrixGate(cnot_matrix())
+def swap_gate(): return MatrixGate(swap_matrix())
+def cz_gate(): return MatrixGate(cz_matrix())
+def toffoli_gate(): return MatrixGate(toffoli_matrix())
