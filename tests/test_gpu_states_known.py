@@ -97,3 +97,23 @@ def test_print():
     assert "State: 2 qubits" in out
     assert "|00⟩ : 0.7071+0.0000i (p=0.5000)" in out
     assert "|11⟩ : 0.7071+0.0000i (p=0.5000)" in out
+
+
+def test_measure_shots_parallel():
+    """tests/test_parallel.rs:144-217"""
+    assert State.zero_state(1).measure_shots_parallel(100) == {0: 100}
+    assert State.one_state(1).measure_shots_parallel(100) == {1: 100}
+    plus = State.plus_state(1).measure_shots_parallel(1000, seed=1)
+    assert set(plus) <= {0, 1} and 0.3 < plus.get(0, 0) / 1000 < 0.7
+    bell = State.bell_state().measure_shots_parallel(200, seed=2)
+    assert bell.get(1, 0) == 0 and bell.get(2, 0) == 0
+    c0, c3 = bell.get(0, 0), bell.get(3, 0)
+    assert c0 > 0 and c3 > 0 and 0.3 < c0 / (c0 + c3) < 0.7
+
+
+def test_normalize_keeps_normalised_state():
+    """tests/test_parallel.rs:38-55"""
+    s = State.zero_state(2)
+    before = float(np.sum(np.abs(s.vector()) ** 2))
+    s.normalize()
+    assert abs(float(np.sum(np.abs(s.vector()) ** 2)) - before) < TOL
