@@ -325,6 +325,12 @@ class Circuit:
             c.close()
         return out
 
+    def execute_and_measure_with_noise(self, seed: int = 0):
+        """execute_and_measure_with_noise (src/circuits/mod.rs:376-411): the same
+        steps as execute_and_measure -- execute already applies the circuit's
+        noise models after every gate."""
+        return self.execute_and_measure(seed)
+
     def __repr__(self):
         # Debug for Circuit (src/circuits/mod.rs:597-608)
         lines = [f"Circuit: {self._name or 'Unnamed Circuit'} ({self._n} qubits)"]

@@ -91,3 +91,11 @@ def test_builder_counts():
     c2.swap(0, 1)
     c2.cz(0, 1)
     assert len(c2.operations()) == 3
+
+
+def test_execute_and_measure_with_noise_delegates(monkeypatch):
+    """execute_and_measure_with_noise takes execute_and_measure's steps (as in
+    src/circuits/mod.rs:376-411), with the seed passed through."""
+    seen = []
+    monkeypatch.setattr(Circuit, "execute_and_measure", lambda self, seed=0: seen.append(seed) or [1])
+    assert Circuit(1).execute_and_measure_with_noise(seed=7) == [1] and seen == [7]
