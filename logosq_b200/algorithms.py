@@ -5,6 +5,7 @@ on the host.
 """
 from __future__ import annotations
 
+import enum
 import math
 
 import numpy as np
@@ -77,8 +78,116 @@ def _h_desc(q):
     return make_desc(abi.H, [q])
 
 
+class RandomGateType(enum.Enum):
+    """RandomGateType (src/algorithms/rqc.rs:11-16)."""
+    Single = 0
+    TwoQubit = 1
+    Rotation = 2
+
+
+class RandomCircuitConfig:
+    """RandomCircuitConfig and its Default (src/algorithms/rqc.rs:19-39): 3
+    qubits, depth 10, gate types Single 0.5 / TwoQubit 0.3 / Rotation 0.2, no
+    seed."""
+
+    def __init__(self, num_qubits=3, depth=10, gate_types=None, seed=None):
+        self.num_qubits, self.depth, self.seed = num_qubits, depth, seed
+        self.gate_types = list(gate_types) if gate_types is not None else [
+            (RandomGateType.Single, 0.5), (RandomGateType.TwoQubit, 0.3),
+            (RandomGateType.Rotation, 0.2)]
+
+
 class rqc:  # noqa: N801
-    """src/algorithms/rqc.rs (random circuits)."""
+    """src/algorithms/rqc.rs (random circuits).
+
+    The generators follow the reference's construction -- per depth step one
+    gate type drawn by weight, then a random qubit (pair), gate and angle, with
+    CZ written as H.CNOT.H and SWAP as three CNOTs -- but draw from the
+    project's SplitMix64 stream: the reference's StdRng (ChaCha12) stream
+    cannot be reproduced here, so equal seeds give the same circuits within
+    this package, not the reference's circuits.  No seed draws one from the
+    operating system, as the reference seeds from entropy.
+    """
+
+    RandomGateType = RandomGateType
+    RandomCircuitConfig = RandomCircuitConfig
+
+    @staticmethod
+    def _rng(seed):
+        import os
+        from .workloads import SplitMix64
+        return SplitMix64(int.from_bytes(os.urandom(8), "little") if seed is None else seed)
+
+    @staticmethod
+    def _select(gate_types, rng):
+        # select_gate_type (rqc.rs:80-95): weighted choice; invalid weights -> Single
+        w = [p for _, p in gate_types]
+        if not w or any(x < 0 or not math.isfinite(x) for x in w) or sum(w) <= 0:
+            return RandomGateType.Single
+        u, acc = rng.uniform() * sum(w), 0.0
+        for (t, p) in gate_types:
+            acc += p
+            if u < acc:
+                return t
+        return gate_types[-1][0]
+
+    @staticmethod
+    def generate(config: RandomCircuitConfig) -> Circuit:
+        """generate (src/algorithms/rqc.rs:42-77)."""
+        n = config.num_qubits
+        c = Circuit(n).with_name(f"Random Circuit (d={config.depth})")
+        rng = rqc._rng(config.seed)
+        for _ in range(config.depth):
+            t = rqc._select(config.gate_types, rng)
+            if t == RandomGateType.TwoQubit and n < 2:
+                t = RandomGateType.Single
+            if t == RandomGateType.Single:
+                q = rng.randint(0, n - 1)
+                (c.h, c.x, c.y, c.z, c.s, c.t)[rng.randint(0, 5)](q)
+            elif t == RandomGateType.TwoQubit:
+                q1 = rng.randint(0, n - 1)
+                q2 = rng.randint(0, n - 1)
+                while q2 == q1:
+                    q2 = rng.randint(0, n - 1)
+                k = rng.randint(0, 2)
+                if k == 0:
+                    c.cnot(q1, q2)
+                elif k == 1:
+                    c.h(q2)
+                    c.cnot(q1, q2)
+                    c.h(q2)
+                else:
+                    c.cnot(q1, q2)
+                    c.cnot(q2, q1)
+                    c.cnot(q1, q2)
+            else:
+                q = rng.randint(0, n - 1)
+                angle = rng.uniform(0.0, 2.0 * math.pi)
+                (c.rx, c.ry, c.rz)[rng.randint(0, 2)](q, angle)
+        return c
+
+    @staticmethod
+    def apply(state, config: RandomCircuitConfig) -> None:
+        """apply (src/algorithms/rqc.rs:185-190)."""
+        rqc.generate(config).execute(state)
+
+    @staticmethod
+    def generate_simple(num_qubits: int, depth: int, seed=None) -> Circuit:
+        """generate_simple (src/algorithms/rqc.rs:194-207): weights 0.4 / 0.4 / 0.2."""
+        return rqc.generate(RandomCircuitConfig(
+            num_qubits, depth, [(RandomGateType.Single, 0.4), (RandomGateType.TwoQubit, 0.4),
+                                (RandomGateType.Rotation, 0.2)], seed))
+
+    @staticmethod
+    def generate_2design(num_qubits: int, seed=None) -> Circuit:
+        """generate_2design (src/algorithms/rqc.rs:211-232): depth 2 n^2, weights
+        0.3 / 0.5 / 0.2.  (The reference takes no seed; the optional one here
+        makes the circuit reproducible.)"""
+        depth = 2 * num_qubits * num_qubits
+        c = rqc.generate(RandomCircuitConfig(
+            num_qubits, depth, [(RandomGateType.Single, 0.3), (RandomGateType.TwoQubit, 0.5),
+                                (RandomGateType.Rotation, 0.2)], seed))
+        return c.with_name(f"2-Design Random Circuit (n={num_qubits}, d={depth})")
 
     @staticmethod
     def generate_supremacy_circuit(num_qubits: int, depth: int, seed: int = 0) -> Circuit:
