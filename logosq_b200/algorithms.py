@@ -210,8 +210,23 @@ class rqc:  # noqa: N801
         return c
 
 
+class HeisenbergParameters:
+    """HeisenbergParameters and its Default (src/algorithms/xyz_heisenberg.rs:8-28)."""
+
+    def __init__(self, jx=1.0, jy=1.0, jz=1.0, external_field=0.0, time_steps=100, dt=0.01):
+        self.jx, self.jy, self.jz = jx, jy, jz
+        self.external_field, self.time_steps, self.dt = external_field, time_steps, dt
+
+
 class xyz_heisenberg:  # noqa: N801
-    """src/algorithms/xyz_heisenberg.rs."""
+    """src/algorithms/xyz_heisenberg.rs.  The reference's functions take a
+    HeisenbergParameters; these accept one in place of the explicit couplings.
+    (calculate_energy, the reference's slow variant, takes an unconjugated
+    product Re sum_i psi_i (P psi)_i per Pauli string, which equals the
+    expectation only for real amplitudes; it is not provided: use
+    calculate_energy_efficient.)"""
+
+    HeisenbergParameters = HeisenbergParameters
 
     @staticmethod
     def hamiltonian(num_qubits, jx, jy, jz, h=0.0) -> PauliObservable:
@@ -239,16 +254,32 @@ class xyz_heisenberg:  # noqa: N801
         return obs
 
     @staticmethod
-    def calculate_energy_efficient(state, jx, jy, jz, external_field=0.0) -> float:
+    def calculate_energy_efficient(state, jx, jy=None, jz=None, external_field=0.0) -> float:
+        """calculate_energy_efficient (src/algorithms/xyz_heisenberg.rs:143-252):
+        (state, params) or (state, jx, jy, jz[, external_field])."""
+        if isinstance(jx, HeisenbergParameters):
+            p = jx
+            jx, jy, jz, external_field = p.jx, p.jy, p.jz, p.external_field
         return xyz_heisenberg.hamiltonian(state.num_qubits(), jx, jy, jz,
                                           external_field).expectation(state)
 
     @staticmethod
-    def create_circuit(num_qubits, jx, jy, jz, external_field, time_steps, dt,
-                       textbook=False) -> Circuit:
+    def simulate(state, params: HeisenbergParameters) -> None:
+        """simulate (src/algorithms/xyz_heisenberg.rs:62-66): the Trotter circuit
+        of create_circuit executed on the state."""
+        xyz_heisenberg.create_circuit(state.num_qubits(), params).execute(state)
+
+    @staticmethod
+    def create_circuit(num_qubits, jx, jy=None, jz=None, external_field=None, time_steps=None,
+                       dt=None, textbook=False) -> Circuit:
         """create_circuit (src/algorithms/xyz_heisenberg.rs:31-59): Trotter steps of
         RXX/RYY/RZZ(2*J*dt) on each bond and RZ(h*dt).  RXX/RYY keep the
-        reference's loop rule unless textbook=True."""
+        reference's loop rule unless textbook=True.  Takes (num_qubits, params)
+        or the explicit couplings."""
+        if isinstance(jx, HeisenbergParameters):
+            p = jx
+            jx, jy, jz, external_field, time_steps, dt = (p.jx, p.jy, p.jz, p.external_field,
+                                                          p.time_steps, p.dt)
         c = Circuit(num_qubits).with_name("XYZ-Heisenberg Model")
         for _ in range(time_steps):
             for i in range(num_qubits - 1):
