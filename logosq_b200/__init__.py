@@ -20,7 +20,7 @@ from .optimization import (Pauli, PauliTerm, PauliObservable, Observable, Ansatz
                            ParameterShift, FiniteDifference, GradientDescent, Adam, LBFGSB,
                            OptimizerResult, VQE, QuantumNaturalGradient)
 from .algorithms import qft, rqc, xyz_heisenberg
-from .qml import VariationalQuantumCircuit, VQCType
+from .qml import DressedVQC, VariationalQuantumCircuit, VQCBuilder, VQCType
 
 __all__ = [
     "abi", "LogosQError", "device_count", "lib", "State", "Gate", "MatrixGate", "gates", "Circuit",
@@ -30,5 +30,5 @@ __all__ = [
     "FiniteDifference", "GradientDescent", "Adam", "LBFGSB", "OptimizerResult", "VQE",
     "QuantumNaturalGradient",
     "qft", "rqc", "xyz_heisenberg",
-    "VariationalQuantumCircuit", "VQCType",
+    "VariationalQuantumCircuit", "VQCType", "VQCBuilder", "DressedVQC",
 ]

@@ -33,6 +33,16 @@ class VariationalQuantumCircuit(Ansatz):
         self.include_input_encoding = include_input_encoding
         self._tpl = None
 
+    @classmethod
+    def new(cls, num_qubits, num_layers) -> "VariationalQuantumCircuit":
+        """VariationalQuantumCircuit::new (src/qml/vqc.rs:84-91): BasicEntangling
+        with the input-encoding layer."""
+        return cls(num_qubits, num_layers)
+
+    @property
+    def num_layers(self):
+        return self.layers
+
     def num_input_params(self):
         return self.n if self.include_input_encoding else 0
 
@@ -105,6 +115,52 @@ class VariationalQuantumCircuit(Ansatz):
 
     def forward_activated(self, inputs, params):
         return [math.tanh(v) for v in self.forward(inputs, params)]
+
+
+class VQCBuilder:
+    """VQCBuilder (src/qml/vqc.rs:26-66): one layer, BasicEntangling and the
+    input-encoding layer unless changed."""
+
+    def __init__(self, num_qubits):
+        self._n, self._layers = num_qubits, 1
+        self._type, self._encoding = VQCType.BasicEntangling, True
+
+    @classmethod
+    def new(cls, num_qubits) -> "VQCBuilder":
+        return cls(num_qubits)
+
+    def with_layers(self, num_layers) -> "VQCBuilder":
+        self._layers = num_layers
+        return self
+
+    def with_type(self, vqc_type) -> "VQCBuilder":
+        self._type = vqc_type
+        return self
+
+    def with_input_encoding(self, include) -> "VQCBuilder":
+        self._encoding = bool(include)
+        return self
+
+    def build(self) -> VariationalQuantumCircuit:
+        return VariationalQuantumCircuit(self._n, self._layers, self._type, self._encoding)
+
+
+class DressedVQC:
+    """DressedVQC (src/qml/vqc.rs:251-284): a VQC with a per-output weight
+    (1.0) and bias (0.0) applied to its outputs."""
+
+    def __init__(self, vqc: VariationalQuantumCircuit, output_size: int):
+        self.vqc = vqc
+        self.output_weights = [1.0] * output_size
+        self.output_biases = [0.0] * output_size
+
+    def forward(self, inputs, params):
+        return [v * w + b for v, w, b in zip(self.vqc.forward(inputs, params),
+                                             self.output_weights, self.output_biases)]
+
+    def num_params(self):
+        return (self.vqc.num_variational_params() + len(self.output_weights)
+                + len(self.output_biases))
 
 
 def check_params(vqc: VariationalQuantumCircuit, params):
