@@ -7,6 +7,7 @@ Each class carries the fields of the reference struct and builds one packed
 from __future__ import annotations
 
 import ctypes as C
+import enum
 import math
 
 import numpy as np
@@ -37,8 +38,37 @@ def make_desc(kind: int, qubits, angles=(), flags: int = 0, matrix=None,
     return d
 
 
+# ---- src/gates/utils.rs: qubit q is bit n-1-q of the basis index ----------
+def qubit_bit_position(qubit: int, num_qubits: int) -> int:
+    return num_qubits - 1 - qubit
+
+
+def qubit_mask(qubit: int, num_qubits: int) -> int:
+    return 1 << qubit_bit_position(qubit, num_qubits)
+
+
+def is_qubit_set(basis_index: int, qubit: int, num_qubits: int) -> bool:
+    return (basis_index & qubit_mask(qubit, num_qubits)) != 0
+
+
+def flip_qubit(basis_index: int, qubit: int, num_qubits: int) -> int:
+    return basis_index ^ qubit_mask(qubit, num_qubits)
+
+
+class RotationAxis(enum.Enum):
+    """RotationAxis (src/gates/parameterized.rs:15-21)."""
+    X = 0
+    Y = 1
+    Z = 2
+
+
 class Gate:
     """Trait `Gate` (src/gates/mod.rs:26-35)."""
+
+    @classmethod
+    def new(cls, *args):
+        """The gate structs' ::new constructors (same arguments as the class)."""
+        return cls(*args)
 
     def descriptor(self) -> np.ndarray:  # pragma: no cover - abstract
         raise NotImplementedError

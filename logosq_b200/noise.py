@@ -39,6 +39,11 @@ def _targets(qubits):
 class NoiseModel:
     """Trait NoiseModel (src/noise/mod.rs:10-16)."""
 
+    @classmethod
+    def new(cls, *args):
+        """The models' ::new constructors (same arguments as the class)."""
+        return cls(*args)
+
     def apply(self, state) -> None:
         raise NotImplementedError
 

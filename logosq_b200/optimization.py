@@ -220,6 +220,14 @@ class Ansatz:
         return None
 
 
+class AnsatzType(enum.Enum):
+    """AnsatzType (src/optimization/ansatz.rs:45-56)."""
+    HardwareEfficient = 0
+    RealAmplitudes = 1
+    EfficientSU2 = 2
+    Custom = 3
+
+
 class EntanglingGate(enum.Enum):
     CNOT = "cnot"
     CZ = "cz"
