@@ -200,6 +200,52 @@ class State:
     def apply_gate(self, gate) -> None:
         gate.apply(self)
 
+    # -- QuantumStateBackend (src/states/backend.rs:14-60), as State implements
+    # it (src/states/mod.rs:394-486): each call applies the gate, then normalises.
+    def _check_backend_qubit(self, *qubits):
+        for q in qubits:
+            if not 0 <= q < self._n:
+                raise LogosQError(abi.LQ_ERR_QUBIT_INDEX,
+                                  f"Invalid qubit index: {q} (must be < {self._n})")
+
+    @staticmethod
+    def _interleaved(matrix, dim):
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128))
+        if m.shape != (dim, dim):
+            raise LogosQError(abi.LQ_ERR_DIMENSION_MISMATCH,
+                              f"Dimension mismatch: expected {dim}, got {m.shape}")
+        return m.view(np.float64).reshape(-1)
+
+    def apply_single_qubit_matrix(self, qubit: int, matrix) -> None:
+        """apply_single_qubit_matrix (src/states/mod.rs:399-439): the 2x2 on one
+        qubit (one device sweep), then normalise."""
+        self._check_backend_qubit(qubit)
+        m = self._interleaved(matrix, 2)
+        call("lq_apply_matrix1", self._h, int(qubit), m.ctypes.data_as(C.POINTER(C.c_double)))
+        self.normalize()
+
+    def apply_two_qubit_matrix(self, control: int, target: int, matrix) -> None:
+        """apply_two_qubit_matrix (src/states/mod.rs:441-457): the 4x4 with
+        `control` as the high bit of its index (as the reference expands it),
+        then normalise."""
+        self._check_backend_qubit(control, target)
+        m = self._interleaved(matrix, 4)
+        call("lq_apply_matrix2", self._h, int(control), int(target),
+             m.ctypes.data_as(C.POINTER(C.c_double)))
+        self.normalize()
+
+    def apply_three_qubit_matrix(self, q1: int, q2: int, q3: int, matrix) -> None:
+        """apply_three_qubit_matrix (src/states/mod.rs:459-469): as in the
+        reference, the matrix is applied to the full state (the qubit indices
+        are not used)."""
+        self.apply_full_matrix(matrix)
+
+    def apply_full_matrix(self, matrix) -> None:
+        """apply_full_matrix (src/states/mod.rs:471-486): the 2^n x 2^n matrix on
+        the device, then normalise."""
+        from .gates import MatrixGate
+        MatrixGate(matrix).apply(self)
+
     def print(self) -> str:
         v = self.vector()
         lines = [f"State: {self._n} qubit{'s' if self._n != 1 else ''}"]
