@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import math
+from typing import Protocol, runtime_checkable
 
 import numpy as np
 
@@ -492,6 +493,14 @@ class OptimizerResult:
         self.num_iterations = num_iterations
         self.convergence_history = convergence_history
         self.converged = converged
+
+
+@runtime_checkable
+class Optimizer(Protocol):
+    """Trait Optimizer (src/optimization/optimizer.rs:17-33); GradientDescent and
+    Adam satisfy it."""
+
+    def minimize(self, f, grad_f, initial_params) -> "OptimizerResult": ...
 
 
 class GradientDescent:

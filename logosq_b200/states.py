@@ -11,8 +11,21 @@ import math
 
 import numpy as np
 
+from typing import Protocol, runtime_checkable
+
 from . import abi
 from ._lib import LogosQError, call, lib
+
+
+@runtime_checkable
+class QuantumStateBackend(Protocol):
+    """Trait QuantumStateBackend (src/states/backend.rs:14-60); State satisfies it."""
+
+    def num_qubits(self) -> int: ...
+    def apply_single_qubit_matrix(self, qubit, matrix) -> None: ...
+    def apply_two_qubit_matrix(self, control, target, matrix) -> None: ...
+    def apply_three_qubit_matrix(self, q1, q2, q3, matrix) -> None: ...
+    def apply_full_matrix(self, matrix) -> None: ...
 
 
 class State:
