@@ -757,7 +757,7 @@ def main():
 
     import torch
     from logosq_b200 import State, abi, replicas, workloads
-    from logosq_b200._lib import call, lib
+    from logosq_b200._lib import call
 
     torch.cuda.set_device(local)
     if ws > 1:

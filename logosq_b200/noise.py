@@ -23,8 +23,6 @@ from __future__ import annotations
 import ctypes as C
 import math
 
-import numpy as np
-
 from ._lib import call
 from .workloads import SplitMix64
 

@@ -9,7 +9,7 @@ import pytest
 import oracle
 from logosq_b200 import State, abi, workloads
 from logosq_b200._lib import call
-from logosq_b200.batch import BatchedParameterShift, heisenberg_batch
+from logosq_b200.batch import heisenberg_batch
 
 pytestmark = pytest.mark.gpu
 

@@ -4,7 +4,6 @@ one gate type per depth step (1 operation, or 3 for the CZ and SWAP
 decompositions), qubits in range, determinism per seed, the weights, the
 single-qubit fallback of two-qubit steps on one qubit, invalid weights falling
 back to single-qubit gates, and the 2-design's depth 2 n^2."""
-import numpy as np
 import pytest
 
 from logosq_b200 import rqc
