@@ -250,7 +250,8 @@ int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dt
                                 void *stream, double *out);
 
 /* ---------------------------------------------------------------------------
- * Gates (src/gates/*.rs) -- each call is one in-place sweep on the state's
+ * Gates (src/gates: single_qubit.rs, two_qubit.rs, three_qubit.rs,
+ * parameterized.rs, matrix.rs) -- each call is one in-place sweep on the state's
  * stream, the drop-in for Gate::apply (src/gates/mod.rs:26-35).
  * ------------------------------------------------------------------------- */
 /* One descriptor; theta may be NULL when no param[] index is used. */
