@@ -117,3 +117,19 @@ def test_emulated_brickwork_at_autotuned_widths(width):
     v = random_state(n, 9)
     _with_width(width, lambda: np.testing.assert_allclose(
         fe.run(n, g, v), oracle.apply_circuit(v.copy(), g), rtol=0, atol=1e-12))
+
+
+from hypothesis import HealthCheck, given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=300, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(n=st.integers(5, 12), width=st.integers(5, 12), count=st.integers(1, 60),
+       seed=st.integers(0, 2**31 - 1))
+def test_planner_property_random_circuits(n, width, count, seed):
+    """Any circuit of the engine's gate kinds, at any qubit count and accepted
+    tile width, is planned and encoded into passes that the kernel emulator runs
+    to the oracle's result."""
+    g = random_circuit(n, count, seed)
+    v = random_state(n, seed % 1000 + 1)
+    _with_width(width, lambda: np.testing.assert_allclose(
+        fe.run(n, g, v), oracle.apply_circuit(v.copy(), g), rtol=0, atol=1e-12))
