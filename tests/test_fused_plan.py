@@ -133,3 +133,42 @@ def test_planner_property_random_circuits(n, width, count, seed):
     v = random_state(n, seed % 1000 + 1)
     _with_width(width, lambda: np.testing.assert_allclose(
         fe.run(n, g, v), oracle.apply_circuit(v.copy(), g), rtol=0, atol=1e-12))
+
+
+PARAM_KINDS = {abi.RX: 1, abi.RY: 1, abi.RZ: 1, abi.PHASE: 1, abi.U3: 3, abi.CRX: 1, abi.CRY: 1,
+               abi.CRZ: 1, abi.CPHASE_PARAM: 1, abi.RXX: 1, abi.RYY: 1, abi.RZZ: 1}
+
+
+def random_bound_circuit(n, count, nparams, seed):
+    """Random circuits whose rotation angles are bound to a parameter vector:
+    angle = theta[param] * scale + offset, as an Ansatz template is described."""
+    rng = workloads.SplitMix64(seed)
+    kinds = list(PARAM_KINDS) + [abi.H, abi.CNOT, abi.CZ, abi.SWAP]
+    recs = []
+    for _ in range(count):
+        kind = kinds[rng.randint(0, len(kinds) - 1)]
+        k = 1 if kind in (abi.RX, abi.RY, abi.RZ, abi.PHASE, abi.U3, abi.H) else 2
+        qs = []
+        while len(qs) < k:
+            q = rng.randint(0, n - 1)
+            if q not in qs:
+                qs.append(q)
+        na = PARAM_KINDS.get(kind, 0)
+        params = [rng.randint(0, nparams - 1) if rng.uniform() < 0.7 else None for _ in range(na)]
+        recs.append(make_desc(kind, qs, [rng.uniform(-1, 1) for _ in range(na)],
+                              params=params or None,
+                              scales=[rng.uniform(-2, 2) for _ in range(na)] or None))
+    return np.concatenate(recs)
+
+
+@settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(n=st.integers(5, 11), width=st.integers(5, 12), count=st.integers(1, 50),
+       nparams=st.integers(1, 12), seed=st.integers(0, 2**31 - 1))
+def test_planner_property_parameter_bound_circuits(n, width, count, nparams, seed):
+    """Parameter-bound gates (the ansatz templates of the VQE paths) are encoded
+    with their angles resolved from theta; the emulated passes match the oracle."""
+    g = random_bound_circuit(n, count, nparams, seed)
+    theta = np.array([workloads.SplitMix64(seed + i).uniform(-3, 3) for i in range(nparams)])
+    v = random_state(n, seed % 1000 + 2)
+    _with_width(width, lambda: np.testing.assert_allclose(
+        fe.run(n, g, v, theta), oracle.apply_circuit(v.copy(), g, theta), rtol=0, atol=1e-12))
