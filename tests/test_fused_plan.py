@@ -172,3 +172,37 @@ def test_planner_property_parameter_bound_circuits(n, width, count, nparams, see
     v = random_state(n, seed % 1000 + 2)
     _with_width(width, lambda: np.testing.assert_allclose(
         fe.run(n, g, v, theta), oracle.apply_circuit(v.copy(), g, theta), rtol=0, atol=1e-12))
+
+
+def _unitary(rng, d):
+    a = np.array([[complex(rng.uniform(-1, 1), rng.uniform(-1, 1)) for _ in range(d)]
+                  for _ in range(d)])
+    q, r = np.linalg.qr(a)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+@settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(n=st.integers(5, 11), width=st.integers(5, 12), count=st.integers(1, 40),
+       seed=st.integers(0, 2**31 - 1))
+def test_planner_property_matrix_gates(n, width, count, seed):
+    """Explicit 2x2 / 4x4 matrices (Circuit::add_single/two_qubit_gate lowered to
+    MATRIX1 / MATRIX2), with and without the renormalising flag of the dense
+    builders, mixed with gate structs."""
+    rng = workloads.SplitMix64(seed)
+    recs = []
+    for _ in range(count):
+        r = rng.uniform()
+        flags = abi.FLAG_RENORM if rng.uniform() < 0.3 else 0
+        if r < 0.35:
+            recs.append(make_desc(abi.MATRIX1, [rng.randint(0, n - 1)], flags=flags,
+                                  matrix=_unitary(rng, 2)))
+        elif r < 0.7:
+            a = rng.randint(0, n - 1)
+            b = (a + 1 + rng.randint(0, n - 2)) % n
+            recs.append(make_desc(abi.MATRIX2, [a, b], flags=flags, matrix=_unitary(rng, 4)))
+        else:
+            recs.append(random_circuit(n, 1, rng.randint(0, 2**31)))
+    g = np.concatenate(recs)
+    v = random_state(n, seed % 1000 + 3)
+    _with_width(width, lambda: np.testing.assert_allclose(
+        fe.run(n, g, v), oracle.apply_circuit(v.copy(), g), rtol=0, atol=1e-12))
