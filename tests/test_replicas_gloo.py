@@ -74,3 +74,21 @@ def test_shard_balance_and_determinism():
 def test_single_process_fallbacks():
     assert replicas.max_over_ranks(3.25) == 3.25
     assert replicas.job_throughput(10.0, 2.0, 4) == 20.0
+
+
+from hypothesis import given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=200, deadline=None)
+@given(costs=st.lists(st.floats(0.0, 1e6, allow_nan=False), min_size=0, max_size=60),
+       world=st.integers(1, 9))
+def test_shard_property(costs, world):
+    """Every instance goes to exactly one rank, and the busiest rank's load is
+    within the longest-processing-time bound: the average load plus the largest
+    single cost."""
+    parts = [replicas.shard_instances(costs, world, r) for r in range(world)]
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(len(costs)))
+    if costs:
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= sum(costs) / world + max(costs) + 1e-9 * (1 + sum(costs))
