@@ -226,7 +226,9 @@ int lq_inner_product(const lq_state *a, const lq_state *b, double out[2]);
 int lq_measure_shots(const lq_state *s, uint64_t n_shots, uint64_t seed, uint64_t *host_out);
 /* sum_t coefficient_t * <P_t> (PauliObservable::expectation,
  * src/optimization/observable.rs:228-232; PauliTerm::expectation :95-147).
- * per_term (optional, may be NULL) receives each term's contribution. */
+ * per_term (optional, may be NULL) receives each term's contribution.  Terms
+ * sharing an X mask are evaluated in one sweep; at most 2000 terms may share
+ * one X mask (LQ_ERR_UNSUPPORTED above that). */
 int lq_expectation_pauli(const lq_state *s, const lq_pauli_term *terms, int nterms,
                          int y_convention, double *out, double *per_term);
 

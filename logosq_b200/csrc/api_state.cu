@@ -454,6 +454,15 @@ int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, 
             }
         }
     }
+    // A group's terms sit in the sweep's dynamic shared memory (24 bytes each,
+    // 48 KB per block without an opt-in): refuse larger groups with a clear error.
+    constexpr size_t kMaxGroupTerms = 2000;
+    for (const auto &gr : groups)
+        if (gr.second.size() > kMaxGroupTerms)
+            return set_error(LQ_ERR_UNSUPPORTED,
+                             "%zu Pauli terms share one X mask; at most %zu per X mask "
+                             "(split the observable)",
+                             gr.second.size(), kMaxGroupTerms);
     const uint64_t N = 1ull << n;
     const int th = 256;
     const int g = red_grid(std::max<uint64_t>(N / 2, 1), th);
