@@ -133,6 +133,39 @@ def run_cpu_baseline(n: int, threads: int, repeats: int = 1):
     return nbytes / best / 1e9, best, len(g)
 
 
+def brickwork_parity(n: int, layers: int, threads: int):
+    """The brickwork's own parity check at n qubits (20 layers, seed 2): the
+    fused device path against the oracle's full run of the same circuit
+    (threaded restatement of the reference loops, bitwise identical to its
+    serial mode).  Reports max-abs per amplitude, the fidelity
+    |<psi_cpu|psi_gpu>|^2, and the oracle's own wall time for the whole circuit
+    (a full-circuit CPU figure beside the sampled one)."""
+    import oracle
+    from logosq_b200 import State, abi, workloads
+    from logosq_b200._lib import call
+    g = workloads.brickwork_u3(n, layers, seed=2)
+    st = State.zero_state(n)
+    try:
+        call("lq_apply_circuit", st.handle, n, abi.gate_ptr(g), len(g), None, 0, abi.EXEC_FUSED)
+        got = st.vector()
+    finally:
+        st.close()
+    fw = C.c_int()
+    call("lq_get_fusion_width", C.byref(fw))
+    oracle.set_threads(threads)
+    t0 = time.perf_counter()
+    want = oracle.apply_circuit(oracle.zero_state(n), g)
+    secs = time.perf_counter() - t0
+    oracle.set_threads(1)
+    max_abs = float(np.abs(got - want).max())
+    fid = float(abs(np.vdot(want, got)) ** 2)
+    return {"qubits": n, "layers": layers, "tile_bits": fw.value, "max_abs": max_abs,
+            "fidelity": fid, "one_minus_fidelity": 1.0 - fid, "bar": 1e-12,
+            "ok": bool(max_abs < 1e-12 and abs(1.0 - fid) < 1e-12),
+            "oracle_s": secs, "oracle_threads": threads,
+            "oracle_gbs": workloads.brickwork_bytes(n, layers) / secs / 1e9}
+
+
 # ---------------------------------------------------------------------------
 def run_vqe_batch(args):
     """Batching form: 256 XYZ-Heisenberg VQE instances, n ~ U{10..20}, BasicEntangling
@@ -693,6 +726,9 @@ def main():
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--parity-qubits", type=int, default=28,
+                    help="brickwork: qubit count of the full-circuit check against the oracle, "
+                         "run with the CPU baseline after the timed region (0 = skip)")
     ap.add_argument("--per-gate-steps", type=int, default=1)
     ap.add_argument("--fusion-width", type=int, default=0,
                     help="tile bits of the fused passes (0 = autotune over 10, 11, 12)")
@@ -895,12 +931,15 @@ def main():
         del pinned
 
     cpu = None
+    parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         gbs, secs, ng = run_cpu_baseline(n, threads)
         cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"{ng} gates of layer 0 ({ng * 2 // 3} U3 + {ng // 3} CNOT) at {n} "
                          f"qubits, threaded restatement of the reference loops, {secs:.1f} s"}
+        if args.parity_qubits:
+            parity = brickwork_parity(args.parity_qubits, layers, threads)
 
     gpu_launches = args.steps * (launches.value + 1)
     line = {"metric": metric, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
@@ -911,6 +950,8 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "per_gate_path": per_gate,
             "gpu_launches": gpu_launches, "clocks": clocks,
             "fused_passes_per_step": passes.value}
+    if parity is not None:
+        line[f"parity_{parity['qubits']}q"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     st.close()

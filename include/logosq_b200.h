@@ -200,8 +200,19 @@ int lq_state_copy(lq_state *dst, const lq_state *src);
 /* out <- |a> (x) |b> (State::tensor_product, src/states/mod.rs:298-314);
  * out must have n_a + n_b qubits. */
 int lq_state_tensor_product(lq_state *out, const lq_state *a, const lq_state *b);
-/* Wait for all work queued on the state's stream. */
+/* Wait for all work queued on the state's stream.  Returns LQ_ERR_TIMEOUT (and
+ * clears the condition) when a kernel's bounded device wait ran out since the
+ * last call; the handle and the CUDA context stay usable, but the amplitudes
+ * that kernel was working on are undefined. */
 int lq_state_synchronize(lq_state *s);
+/* Failure-path check (no reference counterpart; the reference's error surface
+ * is LogosQError, src/error.rs:9-64): queue one kernel on the state's stream
+ * that waits on a shared-memory barrier which nothing ever completes, giving
+ * up after `polls` bounded try-wait polls (1..1048576), exactly as every
+ * pipeline wait in this library gives up after its own bound.  It then raises
+ * the state's timeout flag and returns, so the next lq_state_synchronize
+ * reports LQ_ERR_TIMEOUT.  Touches no amplitude and copies nothing. */
+int lq_check_wait_timeout(lq_state *s, unsigned polls);
 /* Device pointer and CUDA stream (cudaStream_t) of the state, for callers that
  * interoperate with other CUDA code.  The pointer stays owned by the handle. */
 int lq_state_device_ptr(lq_state *s, void **dptr);

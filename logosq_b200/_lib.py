@@ -55,6 +55,7 @@ _PROTOS = {
     "lq_state_tensor_product": (C.c_int, [_P, _P, _P]),
     "lq_apply_dense": (C.c_int, [_P, _PD, C.c_uint64]),
     "lq_state_synchronize": (C.c_int, [_P]),
+    "lq_check_wait_timeout": (C.c_int, [_P, C.c_uint]),
     "lq_state_device_ptr": (C.c_int, [_P, C.POINTER(_P)]),
     "lq_state_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "lq_norm_sqr": (C.c_int, [_P, _PD]),

@@ -50,7 +50,8 @@ def sources() -> list[Path]:
 def _stale(obj: Path, src: Path) -> bool:
     if not obj.exists():
         return True
-    deps = [src] + list(CSRC.glob("*.h")) + list((HERE.parent / "include").glob("*.h"))
+    deps = ([src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) +
+            list((HERE.parent / "include").glob("*.h")))
     return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps)
 
 

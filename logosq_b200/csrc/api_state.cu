@@ -60,6 +60,33 @@ int ensure_prog(lq_state *s, size_t bytes) {
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
+
+// Waits, with the given bound, on an mbarrier phase that never completes (the
+// barrier expects one arrival and gets none; no copy targets it), then raises
+// the timeout flag: the same give-up path as the pipeline waits of the fused
+// and tensor-core passes, exercised without any copy in flight.
+__global__ void k_wait_probe(unsigned *__restrict__ flag, unsigned polls) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t done = 0;
+    for (unsigned it = 0; it < polls && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(0u)
+            : "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !done) atomicOr(flag, kFlagTimeout);
+}
+
 template <class A>
 __device__ __forceinline__ double2 load_amp(const A *v, uint64_t i);
 template <>
@@ -944,6 +971,15 @@ int lq_state_synchronize(lq_state *s) {
         cudaMemset(s->d_flag, 0, sizeof(unsigned));
         return set_error(LQ_ERR_TIMEOUT, "a bounded device wait ran out");
     }
+    return LQ_OK;
+}
+
+int lq_check_wait_timeout(lq_state *s, unsigned polls) {
+    LQ_TRY(check_state(s));
+    if (polls < 1 || polls > (1u << 20))
+        return set_error(LQ_ERR_INVALID_ARG, "polls must be 1..1048576 (got %u)", polls);
+    k_wait_probe<<<1, 32, 0, s->stream>>>(s->d_flag, polls);
+    LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
 }
 

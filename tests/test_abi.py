@@ -73,10 +73,10 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
         _lib.lib()
 
 
-def test_integration_binding_covers_header():
-    """The Rust binding written out for a LogosQ maintainer binds every entry
-    point the header declares."""
-    text = (ROOT / "INTEGRATION.md").read_text()
+def test_rust_binding_covers_header():
+    """The logosq-cuda crate's raw binding (logosq-cuda/src/ffi.rs) declares
+    every entry point the header declares."""
+    text = (ROOT / "logosq-cuda" / "src" / "ffi.rs").read_text()
     bound = set(re.findall(r"pub fn (lq_\w+)\(", text))
     missing = [n for n in declared_functions() if n not in bound]
     assert not missing, missing
