@@ -317,7 +317,12 @@ static uint64_t reg_bits(const GateOp &o) {
     case OP_PERM1: return 1ull << o.t;
     case OP_SWAP:
     case OP_M2: return (1ull << o.b0) | (1ull << o.b1);
-    default: return 0;  // diagonal
+    default: {  // diagonal: free, unless it is a table factor of a real 4x4
+        uint64_t m = 0;
+        if (o.table)
+            for (int k = 0; k < o.npat; ++k) m |= 1ull << o.pat[k];
+        return m;
+    }
     }
 }
 
@@ -466,6 +471,171 @@ static bool single_matrix(const GateOp &g, int &bit, std::complex<double> u[4]) 
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// Real folding.  Every 2x2 unitary has the Euler form of U3
+// (src/gates/parameterized.rs:249-282):
+//     U = w * diag(1, dphi) * [[c, -s], [s, c]] * diag(1, dlam),   c, s >= 0,
+// so a folded pair G (U_x (x) U_y) with G a permutation times phases (CNOT,
+// SWAP, CZ, CPhase, ...) becomes
+//     D_out * (P * (R_x (x) R_y)) * D_in
+// with a REAL 4x4 in the middle (half the FP64 work of a complex 4x4) and two
+// diagonals on the pair's bits.  The diagonals of a register round are merged
+// on the host into one table per run (encode_round), so a brickwork layer
+// costs about 8 + 4 FP64 instructions per amplitude and pair instead of 16.
+// ---------------------------------------------------------------------------
+static int real_fold_mode() {  // 0: complex 4x4; 1: real 4x4; 2: scaled rotations
+    static const int v = [] {
+        const char *e = getenv("LQ_REAL_FOLD");
+        return e ? atoi(e) : 2;
+    }();
+    return v;
+}
+static bool real_fold_enabled() { return real_fold_mode() != 0; }
+
+struct Euler2 {
+    std::complex<double> w, dphi, dlam;
+    double c, s;
+};
+
+static bool euler2(const std::complex<double> u[4], Euler2 &e) {
+    using cd = std::complex<double>;
+    const cd a = u[0], b = u[1], cc = u[2], d = u[3];
+    const double ra = std::abs(a), rb = std::abs(b), rc = std::abs(cc), rd = std::abs(d);
+    if (std::abs(ra * ra + rc * rc - 1.0) > 1e-12 || std::abs(rb - rc) > 1e-12 ||
+        std::abs(ra - rd) > 1e-12)
+        return false;  // not unitary (e.g. a user matrix): keep the complex form
+    constexpr double tiny = 1e-150;
+    e.c = ra;
+    e.s = rc;
+    e.w = ra > tiny ? a / ra : cd(1.0, 0.0);
+    if (rc > tiny && rb > tiny) {
+        e.dphi = (cc / rc) * std::conj(e.w);
+        e.dlam = (-b / rb) * std::conj(e.w);
+    } else {
+        e.dphi = 1.0;
+        e.dlam = rd > tiny ? (d / rd) * std::conj(e.w) : cd(1.0, 0.0);
+    }
+    const cd r[4] = {e.w * e.c, -e.w * e.s * e.dlam, e.w * e.s * e.dphi,
+                     e.w * e.c * e.dphi * e.dlam};
+    for (int k = 0; k < 4; ++k)
+        if (std::abs(r[k] - u[k]) > 1e-14) return false;
+    return true;
+}
+
+// G is a permutation times phases: column c has its one non-zero in row p[c].
+static bool monomial4(const std::complex<double> G[16], int p[4], std::complex<double> g[4]) {
+    int used = 0;
+    for (int c = 0; c < 4; ++c) {
+        int row = -1;
+        for (int r = 0; r < 4; ++r) {
+            if (G[r * 4 + c] == std::complex<double>(0.0, 0.0)) continue;
+            if (row >= 0) return false;
+            row = r;
+        }
+        if (row < 0 || (used >> row & 1)) return false;
+        used |= 1 << row;
+        p[c] = row;
+        g[c] = G[row * 4 + c];
+    }
+    return true;
+}
+
+// Scaled rotation op on bit b: R = [[c, -s], [s, c]] = sigma * R' with R' one
+// FMA per component (form 0: c >= s, x = s/c, sigma = c; form 1: x = c/s,
+// sigma = s).
+static GateOp scaled_rotation(int b, double c, double s, double &sigma) {
+    GateOp g{};
+    g.type = OP_M1;
+    g.t = b;
+    g.srot = true;
+    double r[4];
+    if (c >= s) {
+        const double x = s / c;
+        g.sform = 0;
+        sigma = c;
+        r[0] = 1.0, r[1] = -x, r[2] = x, r[3] = 1.0;
+    } else {
+        const double x = c / s;
+        g.sform = 1;
+        sigma = s;
+        r[0] = x, r[1] = -1.0, r[2] = 1.0, r[3] = x;
+    }
+    for (int k = 0; k < 4; ++k) g.m[2 * k] = r[k], g.m[2 * k + 1] = 0.0;
+    return g;
+}
+
+// D_in, the real middle and D_out of G (U_x (x) U_y) on bits (bx hi, by lo),
+// appended to out in time order; false when the pair does not have that form.
+// Mode 2 writes the middle as two scaled rotations and the permutation (CNOT
+// either way, SWAP or none) as register moves, with the rotations' scales in
+// D_out; mode 1 (or any other permutation) writes it as one real 4x4.
+static bool real_fold(const std::complex<double> G[16], const std::complex<double> ux[4],
+                      const std::complex<double> uy[4], int bx, int by,
+                      std::vector<GateOp> &out) {
+    using cd = std::complex<double>;
+    Euler2 ex, ey;
+    int p[4];
+    cd gv[4];
+    if (!euler2(ux, ex) || !euler2(uy, ey) || !monomial4(G, p, gv)) return false;
+    const double rx[4] = {ex.c, -ex.s, ex.s, ex.c}, ry[4] = {ey.c, -ey.s, ey.s, ey.c};
+    const cd w = ex.w * ey.w;
+    GateOp din{}, mid{}, dout{};
+    din.type = dout.type = OP_DIAG;
+    din.npat = dout.npat = 2;
+    din.pat[0] = dout.pat[0] = by;  // pattern index = (bit bx) << 1 | (bit by)
+    din.pat[1] = dout.pat[1] = bx;
+    din.table = dout.table = true;
+    for (int i = 0; i < 4; ++i) {
+        const cd fi = (i & 2 ? ex.dlam : cd(1.0)) * (i & 1 ? ey.dlam : cd(1.0));
+        din.m[2 * i] = fi.real();
+        din.m[2 * i + 1] = fi.imag();
+        const cd fo = gv[i] * (i & 2 ? ex.dphi : cd(1.0)) * (i & 1 ? ey.dphi : cd(1.0)) * w;
+        dout.m[2 * p[i]] = fo.real();
+        dout.m[2 * p[i] + 1] = fo.imag();
+    }
+    const int pc = p[0] | p[1] << 2 | p[2] << 4 | p[3] << 6;
+    const int P_ID = 0 | 1 << 2 | 2 << 4 | 3 << 6, P_CX = 0 | 1 << 2 | 3 << 4 | 2 << 6,
+              P_XC = 0 | 3 << 2 | 2 << 4 | 1 << 6, P_SW = 0 | 2 << 2 | 1 << 4 | 3 << 6;
+    if (real_fold_mode() == 2 && (pc == P_ID || pc == P_CX || pc == P_XC || pc == P_SW)) {
+        double sx, sy;
+        const GateOp rxo = scaled_rotation(bx, ex.c, ex.s, sx);
+        const GateOp ryo = scaled_rotation(by, ey.c, ey.s, sy);
+        for (int i = 0; i < 8; ++i) dout.m[i] *= sx * sy;
+        out.push_back(din);
+        out.push_back(rxo);
+        out.push_back(ryo);
+        if (pc == P_CX || pc == P_XC) {
+            GateOp cx{};
+            cx.type = OP_PERM1;
+            cx.t = pc == P_CX ? by : bx;
+            cx.nctrl = 1;
+            cx.ctrl[0] = pc == P_CX ? bx : by;
+            out.push_back(cx);
+        } else if (pc == P_SW) {
+            GateOp sw{};
+            sw.type = OP_SWAP;
+            sw.b0 = bx;
+            sw.b1 = by;
+            out.push_back(sw);
+        }
+        out.push_back(dout);
+        return true;
+    }
+    mid.type = OP_M2;
+    mid.real4 = true;
+    mid.b0 = bx;
+    mid.b1 = by;
+    for (int c = 0; c < 4; ++c)      // row p[c] of P R is row c of R = R_x (x) R_y
+        for (int k = 0; k < 4; ++k) {
+            mid.m[2 * (p[c] * 4 + k)] = rx[(c >> 1) * 2 + (k >> 1)] * ry[(c & 1) * 2 + (k & 1)];
+            mid.m[2 * (p[c] * 4 + k) + 1] = 0.0;
+        }
+    out.push_back(din);
+    out.push_back(mid);
+    out.push_back(dout);
+    return true;
+}
+
 static void fold_pairs(std::vector<GateOp> &gops, std::vector<int> &orig, int T) {
     struct Entry {
         GateOp op;
@@ -534,6 +704,12 @@ static void fold_pairs(std::vector<GateOp> &gops, std::vector<int> &orig, int T)
                         M[r * 4 + c] = s;
                     }
                 ex.dead = ey.dead = true;
+                std::vector<GateOp> rf;
+                if (real_fold_enabled() && real_fold(G, ex.u, ey.u, bx, by, rf)) {
+                    for (const GateOp &q : rf) out.push_back(Entry{q, -1, false, false, -1, {}});
+                    open[bx] = open[by] = -1;
+                    continue;
+                }
                 GateOp m{};
                 m.type = OP_M2;
                 m.b0 = bx;
@@ -694,7 +870,12 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
             if (k >= 0) f.cm |= 1 << k;
             else f.gmask |= 1ull << g.ctrl[c];
         }
-        if (g.type == OP_M1) {
+        if (g.type == OP_M1 && g.srot && f.cm == 0 && f.gmask == 0) {
+            f.type = F_R1S;
+            f.k1 = g.sform;
+            coef.push_back(g.sform == 0 ? g.m[4] : g.m[0]);  // x of the form
+            coef.insert(coef.end(), 7, 0.0);
+        } else if (g.type == OP_M1) {
             f.type = f.cm ? F_M1C : F_M1;
             coef.insert(coef.end(), g.m, g.m + 8);
         } else {
@@ -721,19 +902,20 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
     case OP_M2: {
         // register bits ordered k0 < k1 (the kernel unrolls only those pairs):
         // swapping the bits swaps the two bits of the 4x4 row / column index
-        f.type = F_M2;
+        const bool real = g.real4;
+        f.type = real ? F_M2R : F_M2;
         int k0 = reg(g.b0), k1 = reg(g.b1);
-        if (k0 < k1) {
-            coef.insert(coef.end(), g.m, g.m + 32);
-        } else {
+        int sw[4] = {0, 1, 2, 3};
+        if (k0 > k1) {
             std::swap(k0, k1);
-            const int sw[4] = {0, 2, 1, 3};
-            for (int r = 0; r < 4; ++r)
-                for (int c = 0; c < 4; ++c) {
-                    coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2]);
-                    coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2 + 1]);
-                }
+            sw[1] = 2;
+            sw[2] = 1;
         }
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c) {
+                coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2]);
+                if (!real) coef.push_back(g.m[(sw[r] * 4 + sw[c]) * 2 + 1]);
+            }
         f.k0 = k0;
         f.k1 = k1;
         break;
@@ -923,6 +1105,97 @@ static int launch_pass(lq_state *s, int T, int h, const FusedRound *d_rounds, in
     return LQ_OK;
 }
 
+// Encode the ops of one register round.  Diagonals whose bits are all
+// register bits of the round move as early as they commute and each run of them
+// becomes one F_DTAB: a 16-entry table over the register elements, the product
+// of the run's phases, computed on the host.  A run still open at the end of
+// the round is carried into the next round of the pass (`carry`) when its bits
+// are register bits there too, so it joins that round's first table.
+static void encode_round(const std::vector<GateOp> &gops, const std::vector<int> &pass_gates,
+                         const PlannedRound &rd, const int *next_rpos, int h, int T,
+                         std::vector<const GateOp *> &carry, std::vector<FusedOp> &fops,
+                         std::vector<double> &coef, int &mode) {
+    using cd = std::complex<double>;
+    const int m = T - 4;
+    auto reg_in = [&](const int *rpos, int b) {
+        if (!(b < 4 || (b >= h && b < h + m))) return -1;
+        const int lp = local_pos(b, h);
+        for (int k = 0; k < 4; ++k)
+            if (rpos[k] == lp) return k;
+        return -1;
+    };
+    auto reg = [&](int b) { return reg_in(rd.rpos, b); };
+    const bool merge = real_fold_enabled();
+    auto table_in = [&](const int *rpos, const GateOp &g) {
+        if (!merge || g.type != OP_DIAG || g.renorm) return false;
+        for (int k = 0; k < g.npat; ++k)
+            if (reg_in(rpos, g.pat[k]) < 0) return false;
+        for (int k = 0; k < g.nfix; ++k)
+            if (reg_in(rpos, g.fix[k]) < 0) return false;
+        return true;
+    };
+    auto table_ok = [&](const GateOp &g) { return table_in(rd.rpos, g); };
+    std::vector<const GateOp *> L(carry.begin(), carry.end());
+    carry.clear();
+    for (int k : rd.ops) {
+        const GateOp &g = gops[pass_gates[k]];
+        size_t pos = L.size();
+        if (table_ok(g)) {
+            const uint64_t b = op_bits(g);
+            while (pos > 0 && !(op_bits(*L[pos - 1]) & b)) --pos;
+        }
+        L.insert(L.begin() + pos, &g);
+    }
+    std::vector<const GateOp *> pending;
+    uint64_t pbits = 0;
+    auto flush = [&]() {
+        if (pending.empty()) return;
+        cd tab[16];
+        for (int e = 0; e < 16; ++e) tab[e] = 1.0;
+        for (const GateOp *g : pending)
+            for (int e = 0; e < 16; ++e) {
+                bool on = true;
+                for (int k = 0; k < g->nfix; ++k) on = on && ((e >> reg(g->fix[k])) & 1);
+                if (!on) continue;
+                int pidx = 0;
+                for (int k = 0; k < g->npat; ++k) pidx |= ((e >> reg(g->pat[k])) & 1) << k;
+                tab[e] *= cd(g->m[2 * pidx], g->m[2 * pidx + 1]);
+            }
+        FusedOp f{};
+        f.type = F_DTAB;
+        f.coef = (int)coef.size();
+        f.pb0 = f.pb1 = -1;
+        f.param = f.param2 = -1;
+        f.coef_alt = f.coef_alt2 = -1;
+        for (int e = 0; e < 16; ++e) {
+            coef.push_back(tab[e].real());
+            coef.push_back(tab[e].imag());
+        }
+        fops.push_back(f);
+        mode = std::max(mode, 1);
+        pending.clear();
+        pbits = 0;
+    };
+    for (const GateOp *g : L) {
+        if (table_ok(*g)) {
+            pending.push_back(g);
+            pbits |= op_bits(*g);
+            continue;
+        }
+        if (op_bits(*g) & pbits) flush();
+        encode_op(*g, h, m, rd.rpos, fops, coef);
+        const int t = fops.back().type;
+        if (t == F_M2 || t == F_M2R || t == F_R1S) mode = std::max(mode, 1);
+        if (t == F_BLOCK3 || t == F_BLOCK4) mode = 2;
+    }
+    bool keep = next_rpos != nullptr && !pending.empty();
+    for (const GateOp *g : pending) keep = keep && table_in(next_rpos, *g);
+    if (keep)
+        carry = pending;
+    else
+        flush();
+}
+
 // Build the device program of every fused pass of `steps`.
 static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<GateOp> &gops,
                          int T, std::vector<FusedRound> &rounds, std::vector<FusedOp> &fops,
@@ -930,15 +1203,14 @@ static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<G
     for (auto &st : steps) {
         if (!st.fused) continue;
         PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), 0};
-        for (auto &rd : st.pass.rounds) {
+        std::vector<const GateOp *> carry;
+        for (size_t ri = 0; ri < st.pass.rounds.size(); ++ri) {
+            const PlannedRound &rd = st.pass.rounds[ri];
+            const int *next = ri + 1 < st.pass.rounds.size() ? st.pass.rounds[ri + 1].rpos : nullptr;
             FusedRound fr{};
             fill_round(fr, rd.rpos, T, st.pass.h);
             fr.op_begin = (int)fops.size();
-            for (int k : rd.ops) {
-                encode_op(gops[st.pass.gates[k]], st.pass.h, T - 4, rd.rpos, fops, coef);
-                if (fops.back().type == F_M2) pl.mode = std::max(pl.mode, 1);
-                if (fops.back().type >= F_BLOCK3) pl.mode = 2;
-            }
+            encode_round(gops, st.pass.gates, rd, next, st.pass.h, T, carry, fops, coef, pl.mode);
             fr.op_end = (int)fops.size();
             rounds.push_back(fr);
         }

@@ -22,7 +22,11 @@ enum FusedOpType {
     F_SWAP = 5,   // swap reg bits k0, k1
     F_M2 = 6,     // 4x4, index = bit(k0)<<1 | bit(k1)
     F_BLOCK3 = 7, // 8x8 on reg bits 0..2 (matrix bit j <-> reg bit j)
-    F_BLOCK4 = 8  // 16x16 on reg bits 0..3
+    F_BLOCK4 = 8, // 16x16 on reg bits 0..3
+    F_M2R = 9,    // real 4x4 (16 doubles), index = bit(k0)<<1 | bit(k1), k0 < k1
+    F_DTAB = 10,  // amplitude e *= table[e] (16 complex), e = register element index
+    F_R1S = 11    // scaled real rotation on reg bit k0, x = coef[0]:
+                  // k1 = 0: [[1, -x], [x, 1]];  k1 = 1: [[x, -1], [1, x]]
 };
 
 struct FusedOp {
@@ -149,6 +153,69 @@ __device__ __forceinline__ void reg_m2(double2 (&a)[16], const double *__restric
     }
 }
 
+// Real 4x4 on register bits (K0, K1): a complex amplitude vector times a real
+// matrix is two real matrix-vector products, half the FP64 work of a complex
+// 4x4.  The 16 coefficients are read once and serve all four groups.
+template <int K0, int K1>
+__device__ __forceinline__ void reg_m2r(double2 (&a)[16], const double *__restrict__ c) {
+    double m[16];
+#pragma unroll
+    for (int q = 0; q < 16; q += 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(c + q);
+        m[q] = v.x;
+        m[q + 1] = v.y;
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
+        const int i0 = e, i1 = e | (1 << K1), i2 = e | (1 << K0), i3 = e | (1 << K0) | (1 << K1);
+        const double2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+        double2 o[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            o[r].x = fma(m[4 * r + 3], x3.x, fma(m[4 * r + 2], x2.x, fma(m[4 * r + 1], x1.x,
+                                                                          m[4 * r] * x0.x)));
+            o[r].y = fma(m[4 * r + 3], x3.y, fma(m[4 * r + 2], x2.y, fma(m[4 * r + 1], x1.y,
+                                                                          m[4 * r] * x0.y)));
+        }
+        a[i0] = o[0];
+        a[i1] = o[1];
+        a[i2] = o[2];
+        a[i3] = o[3];
+    }
+}
+
+// Scaled real rotation on register bit K: one FMA per real output component,
+// a quarter of a complex 2x2.  FORM 0: y0 = x0 - t x1, y1 = x1 + t x0;
+// FORM 1: y0 = u x0 - x1, y1 = x0 + u x1.  (The scale the host factored out
+// of the rotation travels in a diagonal table.)
+template <int K, int FORM>
+__device__ __forceinline__ void reg_r1s(double2 (&a)[16], double x) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if (e & (1 << K)) continue;
+        const double2 x0 = a[e], x1 = a[e | (1 << K)];
+        if (FORM == 0) {
+            a[e] = make_double2(fma(-x, x1.x, x0.x), fma(-x, x1.y, x0.y));
+            a[e | (1 << K)] = make_double2(fma(x, x0.x, x1.x), fma(x, x0.y, x1.y));
+        } else {
+            a[e] = make_double2(fma(x, x0.x, -x1.x), fma(x, x0.y, -x1.y));
+            a[e | (1 << K)] = make_double2(fma(x, x1.x, x0.x), fma(x, x1.y, x0.y));
+        }
+    }
+}
+
+// Diagonal over the register bits: one complex factor per register element,
+// the product of every diagonal gate of the run (computed on the host).
+__device__ __forceinline__ void reg_dtab(double2 (&a)[16], const double *__restrict__ c) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const double2 p = *reinterpret_cast<const double2 *>(c + 2 * e);
+        const double2 v = a[e];
+        a[e] = make_double2(fma(-v.y, p.y, v.x * p.x), fma(v.x, p.y, v.y * p.x));
+    }
+}
+
 template <int KB>
 __device__ __forceinline__ void reg_block(double2 (&a)[16], const double *__restrict__ c) {
     constexpr int D = 1 << KB;
@@ -269,6 +336,30 @@ __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &
                 case 6: reg_m2<1, 2>(a, cfull); break;
                 case 7: reg_m2<1, 3>(a, cfull); break;
                 default: reg_m2<2, 3>(a, cfull); break;
+                }
+            } else if (op.type == F_M2R) {
+                const int key = op.k0 * 4 + op.k1;
+                switch (key) {
+                case 1: reg_m2r<0, 1>(a, cfull); break;
+                case 2: reg_m2r<0, 2>(a, cfull); break;
+                case 3: reg_m2r<0, 3>(a, cfull); break;
+                case 6: reg_m2r<1, 2>(a, cfull); break;
+                case 7: reg_m2r<1, 3>(a, cfull); break;
+                default: reg_m2r<2, 3>(a, cfull); break;
+                }
+            } else if (op.type == F_DTAB) {
+                reg_dtab(a, cfull);
+            } else if (op.type == F_R1S) {
+                const double x = c8[0];
+                switch (op.k0 * 2 + op.k1) {
+                case 0: reg_r1s<0, 0>(a, x); break;
+                case 1: reg_r1s<0, 1>(a, x); break;
+                case 2: reg_r1s<1, 0>(a, x); break;
+                case 3: reg_r1s<1, 1>(a, x); break;
+                case 4: reg_r1s<2, 0>(a, x); break;
+                case 5: reg_r1s<2, 1>(a, x); break;
+                case 6: reg_r1s<3, 0>(a, x); break;
+                default: reg_r1s<3, 1>(a, x); break;
                 }
             } else if constexpr (MODE >= 2) {
                 if (op.type == F_BLOCK3) reg_block<3>(a, cfull);

@@ -23,6 +23,16 @@ struct GateOp {
     int nfix = 0, fix[2] = {-1, -1};
     int b0 = -1, b1 = -1;        // SWAP / M2
     bool renorm = false;
+    // Fused-path planning hints (other consumers read the op as its type says):
+    // real4: an OP_M2 whose matrix is real (imaginary parts zero);
+    // table: an OP_DIAG on pattern bits only, kept in the register set of the
+    // round that applies it so it joins that round's diagonal table.
+    bool real4 = false;
+    bool table = false;
+    // srot: an OP_M1 that is a scaled real rotation, [[1, -x], [x, 1]] (form 0)
+    // or [[x, -1], [1, x]] (form 1) with x = m[0]; m[] holds the full real 2x2.
+    bool srot = false;
+    int sform = 0;
     double m[32] = {0};          // M1: 8 doubles; M2: 32; DIAG: ph[0..3] as 8 doubles
 };
 

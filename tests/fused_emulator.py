@@ -21,7 +21,7 @@ OP_DT = np.dtype([("type", np.int32), ("k0", np.int32), ("k1", np.int32), ("cm",
                   ("param", np.int32), ("coef_alt", np.int32), ("param2", np.int32),
                   ("coef_alt2", np.int32)], align=True)
 
-F_M1, F_M1C, F_X, F_XC, F_DIAG, F_SWAP, F_M2, F_BLOCK3, F_BLOCK4 = range(9)
+F_M1, F_M1C, F_X, F_XC, F_DIAG, F_SWAP, F_M2, F_BLOCK3, F_BLOCK4, F_M2R, F_DTAB, F_R1S = range(12)
 
 
 def dump(n, gates, theta=None):
@@ -150,5 +150,30 @@ def apply_op(a, op, coef, gbase, gp):
             for rr in range(4):
                 out = sum(M[rr, q] * vin[q] for q in range(4))
                 a[idx[rr]] = np.where(act, out, vin[rr])
+    elif t == F_M2R:
+        M = np.array([c[k] for k in range(16)]).reshape(4, 4)
+        for e in range(16):
+            if (e & (1 << k0)) or (e & (1 << k1)):
+                continue
+            idx = [e, e | (1 << k1), e | (1 << k0), e | (1 << k0) | (1 << k1)]
+            vin = [a[i] for i in idx]
+            for rr in range(4):
+                out = sum(M[rr, q] * vin[q] for q in range(4))
+                a[idx[rr]] = np.where(act, out, vin[rr])
+    elif t == F_R1S:
+        x = c[0]
+        for e in range(16):
+            if e & (1 << k0):
+                continue
+            a0, a1 = a[e], a[e | (1 << k0)]
+            if k1 == 0:
+                n0, n1 = a0 - x * a1, a1 + x * a0
+            else:
+                n0, n1 = x * a0 - a1, a0 + x * a1
+            a[e] = np.where(act, n0, a0)
+            a[e | (1 << k0)] = np.where(act, n1, a1)
+    elif t == F_DTAB:
+        for e in range(16):
+            a[e] = np.where(act, a[e] * cpx(e), a[e])
     else:
         raise NotImplementedError(t)

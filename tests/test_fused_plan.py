@@ -70,13 +70,24 @@ def _two_qubit_layer(n, kind, seed):
                                   abi.RZZ])
 def test_pair_fold_emits_4x4_ops_and_matches_oracle(kind):
     """Single-qubit gates on both bits of a two-qubit gate fold into one 4x4 op
-    (encoded with register bits k0 < k1); the emulated program matches the oracle."""
+    (encoded with register bits k0 < k1); the emulated program matches the oracle.
+    When the two-qubit gate is a permutation times phases (CNOT, CZ, CPhase,
+    SWAP, RZZ) the 4x4 is real (F_M2R) and the Euler phases of the single-qubit
+    gates go into diagonal tables over the round's register bits (F_DTAB)."""
     n = 10
     g = _two_qubit_layer(n, kind, 3)
     _, _, _, ops, _ = fe.dump(n, g)
-    m2 = ops[ops["type"] == fe.F_M2]
-    assert len(m2) == n // 2
-    assert (m2["k0"] < m2["k1"]).all()
+    real = kind in (abi.CNOT, abi.CZ, abi.CPHASE, abi.SWAP, abi.RZZ)
+    if real:
+        # two scaled rotations per pair, their scales and phases in tables
+        assert (ops["type"] == fe.F_R1S).sum() == 2 * (n // 2)
+        assert (ops["type"] == fe.F_DTAB).any()
+        assert not (ops["type"] == fe.F_M2).any()
+    else:
+        m2 = ops[ops["type"] == fe.F_M2]
+        assert len(m2) == n // 2
+        assert (m2["k0"] < m2["k1"]).all()
+        assert not (ops["type"] == fe.F_DTAB).any()
     v = random_state(n, 4)
     assert np.abs(fe.run(n, g, v) - oracle.apply_circuit(v.copy(), g)).max() < 1e-12
 
