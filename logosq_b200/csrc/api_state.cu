@@ -3,7 +3,6 @@
 // Reference: src/states/mod.rs (State, normalize, probabilities,
 // inner_product_parallel, measure*) and src/optimization/observable.rs
 // (PauliTerm::expectation, PauliObservable::expectation).
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cstdarg>
@@ -385,6 +384,89 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     return x ^ (x >> 31);
 }
 
+// ---------------------------------------------------------------------------
+// Cumulative distribution for sampling: a deterministic three-phase FP64
+// inclusive scan with a fixed summation order (so a CPU restatement reproduces
+// every value bit for bit).  A chunk is 1024 values = 256 threads x 4:
+//   s_j    = running sum of the thread's 4 values (left to right);
+//   incl_t = Kogge-Stone inclusive scan of the threads' s_3 inside each warp
+//            (shuffle offsets 1, 2, 4, 8, 16);
+//   W_w    = exclusive running sum of the 8 warp totals (one thread, in order);
+//   cdf    = (W_w + incl_{t-1}) + s_j   (incl_{-1} = 0 at lane 0),
+// and the chunk total is the chunk's last cdf value.  Chunk totals are scanned
+// the same way (recursively) and added as base + value to every later chunk.
+// ---------------------------------------------------------------------------
+constexpr int kScanChunk = 1024;
+
+__global__ void __launch_bounds__(256) k_probs_exact_c128(const double2 *__restrict__ v,
+                                                          double *__restrict__ p, uint64_t N) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 a = v[i];
+        p[i] = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));  // no contraction
+    }
+}
+
+__global__ void __launch_bounds__(256) k_probs_exact_c64(const float2 *__restrict__ v,
+                                                         double *__restrict__ p, uint64_t N) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float2 a = v[i];
+        const double x = a.x, y = a.y;
+        p[i] = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scan_chunks(const double *__restrict__ in,
+                                                     double *__restrict__ out,
+                                                     double *__restrict__ chunk_total,
+                                                     uint64_t N) {
+    __shared__ double W[8];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + 4u * t;
+    double s[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double x = base + j < N ? in[base + j] : 0.0;
+        s[j] = j == 0 ? x : __dadd_rn(s[j - 1], x);
+    }
+    double incl = s[3];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = __dadd_rn(y, incl);
+    }
+    double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = 0.0;
+    if (lane == 31) W[warp] = incl;  // warp total
+    __syncthreads();
+    if (t == 0) {
+        double run = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            const double tot = W[w];
+            W[w] = run;
+            run = __dadd_rn(run, tot);
+        }
+    }
+    __syncthreads();
+    const double off = __dadd_rn(W[warp], excl);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double v = __dadd_rn(off, s[j]);
+        if (base + j < N) out[base + j] = v;
+        if (t == 255 && j == 3) chunk_total[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_scan_add_base(double *__restrict__ cdf, const double *__restrict__ incl_total,
+                                uint64_t N) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x + kScanChunk; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = i / kScanChunk;
+        cdf[i] = __dadd_rn(incl_total[c - 1], cdf[i]);
+    }
+}
+
 __global__ void k_sample(const double *__restrict__ cdf, uint64_t N, uint64_t nshots,
                          uint64_t seed, uint64_t *__restrict__ out) {
     const double total = cdf[N - 1];
@@ -627,6 +709,7 @@ extern "C" {
 int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dtype,
                                 const lq_pauli_term *terms, int nterms, int y_convention,
                                 void *stream, double *out) {
+    clear_error();
     if (!d_amplitudes || !out || (nterms > 0 && !terms) || nterms < 0)
         return set_error(LQ_ERR_INVALID_ARG, "null pointer or negative term count");
     if (num_qubits < 1 || num_qubits > 36)
@@ -651,6 +734,22 @@ int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dt
             return set_error(LQ_ERR_QUBIT_INDEX, "Pauli term %d acts on a qubit >= %d", t, n);
         if (terms[t].ny != __builtin_popcountll(terms[t].xmask & terms[t].zmask))
             return set_error(LQ_ERR_INVALID_ARG, "Pauli term %d: ny does not match its masks", t);
+    }
+    // The scratch array is per device: the amplitudes must be on the current one.
+    {
+        cudaPointerAttributes pa{};
+        int dev = 0;
+        LQ_CUDA_TRY(cudaGetDevice(&dev));
+        if (cudaPointerGetAttributes(&pa, d_amplitudes) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(LQ_ERR_INVALID_ARG, "d_amplitudes is not a CUDA pointer");
+        }
+        if (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)
+            return set_error(LQ_ERR_INVALID_ARG, "d_amplitudes is not device memory");
+        if (pa.device != dev)
+            return set_error(LQ_ERR_INVALID_ARG,
+                             "d_amplitudes is on device %d, the current device is %d", pa.device,
+                             dev);
     }
     unsigned char *scratch = nullptr;
     LQ_TRY(static_scratch_address(&scratch));
@@ -1093,29 +1192,53 @@ int lq_inner_product(const lq_state *a, const lq_state *b, double out[2]) {
     return LQ_OK;
 }
 
+// Inclusive scan of in[0..N) into out (the fixed-order scan above); tot holds
+// the chunk totals of every level (ceil(N/1024) + ceil(N/2^20) + ... doubles).
+static int scan_inclusive(const double *in, double *out, double *tot, uint64_t N,
+                          cudaStream_t st) {
+    const uint64_t nc = (N + kScanChunk - 1) / kScanChunk;
+    if (nc > 0x7fffffffull) return set_error(LQ_ERR_UNSUPPORTED, "scan too long");
+    k_scan_chunks<<<(unsigned)nc, 256, 0, st>>>(in, out, tot, N);
+    LQ_CUDA_TRY(cudaGetLastError());
+    if (nc > 1) {
+        double *incl = tot + nc;  // scanned chunk totals, in place after the totals
+        LQ_TRY(scan_inclusive(tot, incl, incl + nc, nc, st));
+        k_scan_add_base<<<grid_for(N, 256), 256, 0, st>>>(out, incl, N);
+        LQ_CUDA_TRY(cudaGetLastError());
+    }
+    return LQ_OK;
+}
+
+static uint64_t scan_scratch(uint64_t N) {  // doubles needed by scan_inclusive's tot
+    uint64_t need = 0;
+    for (uint64_t n = N; n > 1;) {
+        const uint64_t nc = (n + kScanChunk - 1) / kScanChunk;
+        need += 2 * nc;
+        n = nc;
+    }
+    return need + 2;
+}
+
 int lq_measure_shots(const lq_state *s, uint64_t n_shots, uint64_t seed, uint64_t *host_out) {
     LQ_TRY(check_state(s));
     if (!host_out && n_shots) return set_error(LQ_ERR_INVALID_ARG, "null output");
     if (n_shots == 0) return LQ_OK;
     const uint64_t N = 1ull << s->n;
-    double *p = nullptr, *cdf = nullptr;
+    double *p = nullptr, *cdf = nullptr, *tot = nullptr;
     uint64_t *d_out = nullptr;
-    void *tmp = nullptr;
-    size_t tmp_bytes = 0;
     LQ_CUDA_TRY(cudaMallocAsync(&p, N * 8, s->stream));
     LQ_CUDA_TRY(cudaMallocAsync(&cdf, N * 8, s->stream));
+    LQ_CUDA_TRY(cudaMallocAsync(&tot, scan_scratch(N) * 8, s->stream));
     LQ_CUDA_TRY(cudaMallocAsync(&d_out, n_shots * 8, s->stream));
     if (s->dtype == LQ_C128)
-        k_probs<<<grid_for(N, 256), 256, 0, s->stream>>>((const double2 *)s->d, p, N);
+        k_probs_exact_c128<<<grid_for(N, 256), 256, 0, s->stream>>>((const double2 *)s->d, p, N);
     else
-        k_probs<<<grid_for(N, 256), 256, 0, s->stream>>>((const float2 *)s->d, p, N);
-    LQ_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, p, cdf, (int64_t)N, s->stream));
-    LQ_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, s->stream));
-    LQ_CUDA_TRY(cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, p, cdf, (int64_t)N, s->stream));
+        k_probs_exact_c64<<<grid_for(N, 256), 256, 0, s->stream>>>((const float2 *)s->d, p, N);
+    LQ_TRY(scan_inclusive(p, cdf, tot, N, s->stream));
     k_sample<<<grid_for(n_shots, 256), 256, 0, s->stream>>>(cdf, N, n_shots, seed, d_out);
     LQ_CUDA_TRY(cudaGetLastError());
     LQ_CUDA_TRY(cudaMemcpyAsync(host_out, d_out, n_shots * 8, cudaMemcpyDeviceToHost, s->stream));
-    LQ_CUDA_TRY(cudaFreeAsync(tmp, s->stream));
+    LQ_CUDA_TRY(cudaFreeAsync(tot, s->stream));
     LQ_CUDA_TRY(cudaFreeAsync(p, s->stream));
     LQ_CUDA_TRY(cudaFreeAsync(cdf, s->stream));
     LQ_CUDA_TRY(cudaFreeAsync(d_out, s->stream));

@@ -274,3 +274,81 @@ def noise_phase_damping(psi, lam: float, qubits):
         new = psi.copy()
         new[((idx >> q) & 1) == 1] *= math.sqrt(1.0 - lam)
     return new / np.sqrt(np.sum(np.abs(new) ** 2))
+
+
+# ---------------------------------------------------------------------------
+# Shot sampling.  The reference's measure (src/states/mod.rs:180-185) and
+# measure_shots_parallel (:244-258) draw each shot with rand 0.8's WeightedIndex:
+# the running sums of |psi_i|^2, a uniform u in [0, total), and the first index
+# whose running sum exceeds u.  The engine keeps that rule with its own
+# counter-based uniforms (SplitMix64 of the shot number) and running sums in a
+# fixed parallel order; this restatement reproduces both bit for bit, so the
+# sampled indices can be compared exactly.
+# ---------------------------------------------------------------------------
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        x = (x + np.uint64(0x9E3779B97F4A7C15)) & _M64
+        x = ((x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & _M64
+        x = ((x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & _M64
+        return x ^ (x >> np.uint64(31))
+
+
+def _scan_chunks(v: np.ndarray):
+    """One level of the engine's fixed-order inclusive scan: chunks of 1024
+    values, 256 threads x 4 running sums, a Kogge-Stone scan of the thread
+    totals inside each 32-lane warp, an in-order exclusive scan of the 8 warp
+    totals, cdf = (W_warp + incl_{t-1}) + s_j."""
+    N = len(v)
+    nc = -(-N // 1024)
+    x = np.zeros(nc * 1024)
+    x[:N] = v
+    x = x.reshape(nc, 8, 32, 4)
+    s = np.cumsum(x, axis=3)                       # sequential, left to right
+    incl = s[..., 3].copy()                        # (nc, 8, 32)
+    for off in (1, 2, 4, 8, 16):
+        old = incl.copy()
+        incl[..., off:] = old[..., :-off] + old[..., off:]
+    excl = np.zeros_like(incl)
+    excl[..., 1:] = incl[..., :-1]
+    wt = incl[..., 31]                             # (nc, 8) warp totals
+    W = np.zeros_like(wt)
+    run = np.zeros(nc)
+    for w in range(8):
+        W[:, w] = run
+        run = run + wt[:, w]
+    off = W[..., None] + excl                      # (nc, 8, 32)
+    cdf = off[..., None] + s
+    cdf = cdf.reshape(-1)
+    return cdf[:N], cdf.reshape(nc, 1024)[:, -1].copy()
+
+
+def sampling_cdf(psi: np.ndarray) -> np.ndarray:
+    """The engine's cumulative probabilities of psi, value for value."""
+    p = psi.real * psi.real + psi.imag * psi.imag   # two products, one sum: no FMA
+    return _scan(p)
+
+
+def _scan(v: np.ndarray) -> np.ndarray:
+    """Chunk scans, chunk totals scanned the same way, base + value."""
+    cdf, tot = _scan_chunks(v)
+    if len(tot) > 1:
+        incl = _scan(tot)
+        c = np.arange(len(cdf)) // 1024
+        later = c >= 1
+        cdf[later] = incl[c[later] - 1] + cdf[later]
+    return cdf
+
+
+def sample_indices(psi: np.ndarray, n_shots: int, seed: int) -> np.ndarray:
+    """Shot s draws u = (r >> 11) * 2^-53 * total with r = SplitMix64(seed xor
+    SplitMix64(s)) and returns the first index whose running sum exceeds u."""
+    cdf = sampling_cdf(np.ascontiguousarray(psi, dtype=np.complex128))
+    total = cdf[-1]
+    s = np.arange(n_shots, dtype=np.uint64)
+    r = _splitmix64(np.uint64(seed) ^ _splitmix64(s))
+    u = (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) * total
+    idx = np.searchsorted(cdf, u, side="right")
+    return np.minimum(idx, len(cdf) - 1).astype(np.uint64)

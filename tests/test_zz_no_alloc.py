@@ -39,12 +39,12 @@ def _regular(st, terms, yconv):
     return out.value
 
 
-def _static(st, terms, yconv):
+def _static(st, terms, yconv, dtype=abi.LQ_C128):
     ptr, stream = C.c_void_p(), C.c_void_p()
     call("lq_state_device_ptr", st.handle, C.byref(ptr))
     call("lq_state_stream", st.handle, C.byref(stream))
     out = C.c_double()
-    call("lq_expectation_pauli_static", ptr, st.num_qubits(), abi.LQ_C128, abi.term_ptr(terms),
+    call("lq_expectation_pauli_static", ptr, st.num_qubits(), dtype, abi.term_ptr(terms),
          len(terms), yconv, stream, C.byref(out))
     return out.value
 
@@ -67,3 +67,49 @@ def test_static_expectation_rejects_too_many_terms():
     with pytest.raises(LogosQError) as e:
         _static(st, terms, abi.Y_REFERENCE)
     assert e.value.code == abi.LQ_ERR_UNSUPPORTED
+
+
+def test_static_expectation_matches_oracle():
+    """Against the oracle's restatement of PauliTerm::expectation
+    (src/optimization/observable.rs:95-147), not only against the engine:
+    X-mask-0 terms and X-mask groups, both Y conventions, small and large n,
+    and exactly the 1024-term limit."""
+    import oracle
+    for n, count, seed, yconv in [(2, 12, 5, abi.Y_REFERENCE), (13, 200, 6, abi.Y_TEXTBOOK),
+                                  (16, 1024, 7, abi.Y_REFERENCE)]:
+        v = workloads.gaussian_state(n, seed)
+        terms = _terms(n, count, seed)
+        st = State.zero_state(n)
+        try:
+            st.set_vector(v)
+            got = _static(st, terms, yconv)
+        finally:
+            st.close()
+        want = oracle.expectation(v, terms, yconv)
+        assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (n, count, got, want)
+
+
+def test_static_expectation_complex64_state():
+    """A complex64 state (the precision form's storage): same value as the
+    regular entry point on the same state, within FP64-accumulation noise."""
+    n = 14
+    st = State.zero_state(n, dtype=abi.LQ_C64)
+    try:
+        st.set_vector(workloads.gaussian_state(n, 3))
+        terms = _terms(n, 90, 4)
+        want = _regular(st, terms, abi.Y_REFERENCE)
+        got = _static(st, terms, abi.Y_REFERENCE, dtype=abi.LQ_C64)
+    finally:
+        st.close()
+    assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (got, want)
+
+
+def test_static_expectation_rejects_host_pointer():
+    """A host buffer is not device memory: refused before any kernel runs."""
+    buf = np.zeros(2 * 16, dtype=np.float64)
+    out = C.c_double()
+    terms = _terms(4, 3, 1)
+    with pytest.raises(LogosQError) as e:
+        call("lq_expectation_pauli_static", buf.ctypes.data_as(C.c_void_p), 4, abi.LQ_C128,
+             abi.term_ptr(terms), len(terms), abi.Y_REFERENCE, None, C.byref(out))
+    assert e.value.code == abi.LQ_ERR_INVALID_ARG
