@@ -39,6 +39,17 @@ FALLBACK_HBM = 6650.0  # GB/s, earlier measurement on this pool
 FP64_PEAK_TFLOPS = 36.6  # dependent-chain-free DFMA throughput measured on this pool's B200
 
 
+def ncu_traffic(kernel: str, n: int):
+    """DRAM bytes per launch of `kernel` at n qubits, scaled from the committed
+    single-kernel ncu capture (the launch sweeps the whole state, so traffic
+    grows as 2^n); (None, None) when no capture is recorded."""
+    try:
+        d = json.loads((ROOT / "profiles" / "ncu_traffic.json").read_text())[kernel]
+        return float(d["bytes_per_launch"]) * 2.0 ** (n - int(d["qubits"])), int(d["qubits"])
+    except Exception:
+        return None, None
+
+
 def hbm_peak():
     try:
         d = json.loads(PEAKS_FILE.read_text())
@@ -867,9 +878,7 @@ def main():
     peak, peak_kind = hbm_peak()
     fused_launch_ms = fused_ms.value / max(fused_n.value, 1)
     achieved = 2 * S / (fused_launch_ms / 1e3) / 1e9 if fused_n.value else None
-    # ncu (profiles/k_fused_pass_brickwork26q.md): dram read + write per launch at 26
-    # qubits = 2.11e9 B (0.98 x 2S); a launch sweeps the whole state, so scale by 2^(n-26).
-    traffic = 2.11e9 * 2.0 ** (n - 26)
+    traffic, traffic_q = ncu_traffic("k_fused_pass", n)
     n_u3 = int(np.sum(gates["kind"] == abi.U3))
     fp64_flops_step = 14.0 * n_u3 * (1 << n)  # 2x2 complex matrix: 14 flops per amplitude
     roofline = {"kernel": "k_fused_pass (TMA-staged 2^T-amplitude tiles)", "bound": "hbm",
@@ -879,13 +888,13 @@ def main():
                 "launches_per_step": passes.value,
                 "traffic": traffic,
                 "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                "captured at 26 qubits and scaled by 2^(n-26)",
+                                f"captured at {traffic_q} qubits and scaled by 2^(n-{traffic_q})",
                 "fp64": {"achieved_tflops": fp64_flops_step / (ms_step / 1e3) / 1e12,
                          "peak_tflops": FP64_PEAK_TFLOPS,
                          "frac": fp64_flops_step / (ms_step / 1e3) / 1e12 / FP64_PEAK_TFLOPS,
                          "peak_source": "DFMA throughput probe on this pool's B200",
                          "flops_per_step": fp64_flops_step,
-                         "note": "the fused kernel is FP64 / issue bound (profiles/)"}}
+                         "note": "the fused kernel is FP64 / issue bound"}}
 
     # ---- per-gate (unfused) path: one sweep per gate, as Gate::apply --------
     per_gate = None

@@ -183,6 +183,21 @@ __global__ void k_scale_by_norm(A *__restrict__ v, uint64_t N, const double *nor
     }
 }
 
+// v *= sqrt(target / current) (both squared norms, FP64, on the device).
+template <class A>
+__global__ void k_scale_to_norm(A *__restrict__ v, uint64_t N, const double *target_sq,
+                                const double *current_sq) {
+    if (!(*current_sq > 0.0) || !(*target_sq > 0.0)) return;
+    const double f = sqrt(*target_sq / *current_sq);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        A a = v[i];
+        a.x = (decltype(a.x))(a.x * f);
+        a.y = (decltype(a.y))(a.y * f);
+        v[i] = a;
+    }
+}
+
 template <class A>
 __global__ void k_set_basis(A *__restrict__ v, uint64_t N, uint64_t idx) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
@@ -522,6 +537,27 @@ int normalize_impl(lq_state *s) {
         k_scale_by_norm<<<grid_for(N, 256), 256, 0, s->stream>>>((double2 *)s->d, N, d_norm);
     else
         k_scale_by_norm<<<grid_for(N, 256), 256, 0, s->stream>>>((float2 *)s->d, N, d_norm);
+    LQ_CUDA_TRY(cudaGetLastError());
+    return LQ_OK;
+}
+
+// FP64 norm bookkeeping of the precision form: remember the squared norm now,
+// and later scale the state back to it (two slots at the end of the reduction
+// scratch, clear of the partial sums and of normalize's slot).
+int norm_snapshot(lq_state *s) {
+    double *d_in = s->d_red + kRedBlocks * 2 * kMaxTermsPerPass - 2;
+    return norm_sqr_device(s, d_in);
+}
+
+int norm_restore(lq_state *s) {
+    double *d_in = s->d_red + kRedBlocks * 2 * kMaxTermsPerPass - 2;
+    double *d_now = s->d_red + kRedBlocks * 2 * kMaxTermsPerPass - 3;
+    LQ_TRY(norm_sqr_device(s, d_now));
+    const uint64_t N = 1ull << s->n;
+    if (s->dtype == LQ_C128)
+        k_scale_to_norm<<<grid_for(N, 256), 256, 0, s->stream>>>((double2 *)s->d, N, d_in, d_now);
+    else
+        k_scale_to_norm<<<grid_for(N, 256), 256, 0, s->stream>>>((float2 *)s->d, N, d_in, d_now);
     LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
 }

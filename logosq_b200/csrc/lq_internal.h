@@ -100,6 +100,9 @@ int gate_class(int kind);
 
 // api_state.cu
 int normalize_impl(lq_state *s);
+// Record the state's FP64 squared norm; later rescale the state to it.
+int norm_snapshot(lq_state *s);
+int norm_restore(lq_state *s);
 int expectation_impl(const lq_state *s, const lq_pauli_term *terms, int nterms, int yconv,
                      double *out, double *per_term);
 

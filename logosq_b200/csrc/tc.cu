@@ -51,6 +51,14 @@ struct TcBlock {
     uint32_t col_bits[32];  // tile-local index bits of block column c (its 5 bits placed)
 };
 
+static bool tc_restore_norm() {
+    static const int v = [] {
+        const char *e = getenv("LQ_TC_RENORM");
+        return e ? atoi(e) : 1;
+    }();
+    return v != 0;
+}
+
 struct TcPass {
     int32_t h;
     int32_t block_begin, nblocks;
@@ -650,11 +658,18 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
                                          (int)kTcSmem));
         attr = true;
     }
+    // FP32 accumulation in the tensor cores rounds every block's sums toward
+    // zero, which shrinks the state by a near-uniform factor per block; the
+    // FP64 norm of the input is restored at the end of the circuit (one
+    // reduction before, one reduction and one scaling sweep after).
+    const bool restore = tc_restore_norm() && !blocks.empty();
+    if (restore) LQ_TRY(norm_snapshot(s));
     int launches = 0;
     for (size_t si = 0; si < steps.size(); ++si) {
         const PlanStep &st = steps[si];
         if (!st.fused) {
             LQ_TRY(launch_gate_op(s, gops[st.gate]));
+            if (restore && gops[st.gate].renorm) LQ_TRY(norm_snapshot(s));
             continue;
         }
         const TcPass &tp = passes[step_pass[si]];
@@ -668,6 +683,7 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
         LQ_CUDA_TRY(cudaGetLastError());
         ++launches;
     }
+    if (restore) LQ_TRY(norm_restore(s));
     if (nblocks_out) *nblocks_out = (int)blocks.size();
     if (npasses_out) *npasses_out = launches;
     return LQ_OK;

@@ -56,10 +56,14 @@ def job_throughput(units_per_rank: float, max_seconds: float, world_size: int) -
     return world_size * units_per_rank / max_seconds
 
 
-def instance_cost(n: int, nparams: int) -> float:
-    """Relative cost of one VQE instance on the batched engine: 2P+1 circuits
-    over 2^n amplitudes."""
-    return float((2 * nparams + 1) << n)
+def instance_cost(n: int, nparams: int, ngates: int | None = None) -> float:
+    """Relative cost of one VQE instance on the batched engine: 2P+1 circuits,
+    each ngates sweeps over 2^n amplitudes.  ngates defaults to the
+    BasicEntangling ansatz at L = 4 (src/qml/vqc.rs:158-170): RY and RZ on every
+    qubit plus an (n-1)-CNOT ladder per layer, 4(2n + n - 1) = 12n - 4 gates."""
+    if ngates is None:
+        ngates = 12 * n - 4
+    return float((2 * nparams + 1) * ngates) * float(1 << n)
 
 
 def shard_instances(costs, world_size: int, rank: int) -> list[int]:

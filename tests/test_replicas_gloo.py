@@ -92,3 +92,12 @@ def test_shard_property(costs, world):
     if costs:
         loads = [sum(costs[i] for i in p) for p in parts]
         assert max(loads) <= sum(costs) / world + max(costs) + 1e-9 * (1 + sum(costs))
+
+
+def test_instance_cost_counts_gates():
+    """Cost = (2P + 1) circuits x (12n - 4) gates x 2^n amplitudes: a 20-qubit
+    chain weighs (321 * 236 * 2^20) / (161 * 116 * 2^10) times a 10-qubit one."""
+    from logosq_b200 import replicas
+    r = replicas.instance_cost(20, 160) / replicas.instance_cost(10, 80)
+    assert abs(r - (321 * 236 * 2 ** 20) / (161 * 116 * 2 ** 10)) < 1e-9
+    assert replicas.instance_cost(10, 80, ngates=1) == 161 * 2 ** 10
