@@ -596,27 +596,50 @@ static bool real_fold(const std::complex<double> G[16], const std::complex<doubl
     const int pc = p[0] | p[1] << 2 | p[2] << 4 | p[3] << 6;
     const int P_ID = 0 | 1 << 2 | 2 << 4 | 3 << 6, P_CX = 0 | 1 << 2 | 3 << 4 | 2 << 6,
               P_XC = 0 | 3 << 2 | 2 << 4 | 1 << 6, P_SW = 0 | 2 << 2 | 1 << 4 | 3 << 6;
-    if (real_fold_mode() == 2 && (pc == P_ID || pc == P_CX || pc == P_XC || pc == P_SW)) {
+    if (real_fold_mode() >= 2 && (pc == P_ID || pc == P_CX || pc == P_XC || pc == P_SW)) {
         double sx, sy;
         const GateOp rxo = scaled_rotation(bx, ex.c, ex.s, sx);
         const GateOp ryo = scaled_rotation(by, ey.c, ey.s, sy);
         for (int i = 0; i < 8; ++i) dout.m[i] *= sx * sy;
         out.push_back(din);
-        out.push_back(rxo);
-        out.push_back(ryo);
-        if (pc == P_CX || pc == P_XC) {
-            GateOp cx{};
-            cx.type = OP_PERM1;
-            cx.t = pc == P_CX ? by : bx;
-            cx.nctrl = 1;
-            cx.ctrl[0] = pc == P_CX ? bx : by;
-            out.push_back(cx);
-        } else if (pc == P_SW) {
-            GateOp sw{};
-            sw.type = OP_SWAP;
-            sw.b0 = bx;
-            sw.b1 = by;
-            out.push_back(sw);
+        if (real_fold_mode() == 3) {  // separate ops (kept for measurement)
+            out.push_back(rxo);
+            out.push_back(ryo);
+            if (pc == P_CX || pc == P_XC) {
+                GateOp cx{};
+                cx.type = OP_PERM1;
+                cx.t = pc == P_CX ? by : bx;
+                cx.nctrl = 1;
+                cx.ctrl[0] = pc == P_CX ? bx : by;
+                out.push_back(cx);
+            } else if (pc == P_SW) {
+                GateOp sw{};
+                sw.type = OP_SWAP;
+                sw.b0 = bx;
+                sw.b1 = by;
+                out.push_back(sw);
+            }
+        } else {  // one op: both rotations and the permutation
+            GateOp pr{};
+            pr.type = OP_M2;
+            pr.real4 = true;
+            pr.pairrot = true;
+            pr.b0 = bx;
+            pr.b1 = by;
+            pr.px[0] = rxo.sform == 0 ? rxo.m[4] : rxo.m[0];
+            pr.px[1] = ryo.sform == 0 ? ryo.m[4] : ryo.m[0];
+            pr.pf[0] = rxo.sform;
+            pr.pf[1] = ryo.sform;
+            pr.pperm = pc == P_ID ? 0 : pc == P_CX ? 1 : pc == P_XC ? 2 : 3;
+            // the full real matrix P (R'x (x) R'y) for every other reader of the op
+            for (int c = 0; c < 4; ++c)
+                for (int k = 0; k < 4; ++k) {
+                    const double v = rxo.m[2 * ((c >> 1) * 2 + (k >> 1))] *
+                                     ryo.m[2 * ((c & 1) * 2 + (k & 1))];
+                    pr.m[2 * (p[c] * 4 + k)] = v;
+                    pr.m[2 * (p[c] * 4 + k) + 1] = 0.0;
+                }
+            out.push_back(pr);
         }
         out.push_back(dout);
         return true;
@@ -900,6 +923,26 @@ void encode_op(const GateOp &g, int h, int m, const int rpos[4], std::vector<Fus
         coef.insert(coef.end(), 8, 0.0);
         break;
     case OP_M2: {
+        if (g.pairrot) {
+            // F_PAIR: k0 < k1; the op's bit b0 is index bit 1 of its permutation
+            int kb0 = reg(g.b0), kb1 = reg(g.b1);
+            int f0 = g.pf[0], f1 = g.pf[1], perm = g.pperm;
+            double x0 = g.px[0], x1 = g.px[1];
+            if (kb0 > kb1) {  // roles swap: CNOT directions swap, SWAP / none stay
+                std::swap(kb0, kb1);
+                std::swap(f0, f1);
+                std::swap(x0, x1);
+                if (perm == 1 || perm == 2) perm = 3 - perm;
+            }
+            f.type = F_PAIR;
+            f.k0 = kb0;
+            f.k1 = kb1;
+            f.cm = f0 | f1 << 1 | perm << 2;
+            coef.push_back(x0);
+            coef.push_back(x1);
+            coef.insert(coef.end(), 6, 0.0);
+            break;
+        }
         // register bits ordered k0 < k1 (the kernel unrolls only those pairs):
         // swapping the bits swaps the two bits of the 4x4 row / column index
         const bool real = g.real4;
@@ -1185,7 +1228,7 @@ static void encode_round(const std::vector<GateOp> &gops, const std::vector<int>
         if (op_bits(*g) & pbits) flush();
         encode_op(*g, h, m, rd.rpos, fops, coef);
         const int t = fops.back().type;
-        if (t == F_M2 || t == F_M2R || t == F_R1S) mode = std::max(mode, 1);
+        if (t == F_M2 || t == F_M2R || t == F_R1S || t == F_PAIR) mode = std::max(mode, 1);
         if (t == F_BLOCK3 || t == F_BLOCK4) mode = 2;
     }
     bool keep = next_rpos != nullptr && !pending.empty();

@@ -25,8 +25,11 @@ enum FusedOpType {
     F_BLOCK4 = 8, // 16x16 on reg bits 0..3
     F_M2R = 9,    // real 4x4 (16 doubles), index = bit(k0)<<1 | bit(k1), k0 < k1
     F_DTAB = 10,  // amplitude e *= table[e] (16 complex), e = register element index
-    F_R1S = 11    // scaled real rotation on reg bit k0, x = coef[0]:
+    F_R1S = 11,   // scaled real rotation on reg bit k0, x = coef[0]:
                   // k1 = 0: [[1, -x], [x, 1]];  k1 = 1: [[x, -1], [1, x]]
+    F_PAIR = 12   // scaled rotations on reg bits k1 (x = coef[1], form cm bit 1) and
+                  // k0 (x = coef[0], form cm bit 0), then a permutation of the pair
+                  // (cm >> 2: 0 none, 1 CNOT k0 -> k1, 2 CNOT k1 -> k0, 3 SWAP)
 };
 
 struct FusedOp {
@@ -205,6 +208,53 @@ __device__ __forceinline__ void reg_r1s(double2 (&a)[16], double x) {
     }
 }
 
+template <int FORM>
+__device__ __forceinline__ void rot_s(double2 &y0, double2 &y1, double x) {
+    const double2 x0 = y0, x1 = y1;
+    if (FORM == 0) {
+        y0 = make_double2(fma(-x, x1.x, x0.x), fma(-x, x1.y, x0.y));
+        y1 = make_double2(fma(x, x0.x, x1.x), fma(x, x0.y, x1.y));
+    } else {
+        y0 = make_double2(fma(x, x0.x, -x1.x), fma(x, x0.y, -x1.y));
+        y1 = make_double2(fma(x, x1.x, x0.x), fma(x, x1.y, x0.y));
+    }
+}
+
+// A folded pair in real form: rotation on K1, rotation on K0, then the pair's
+// permutation P written as the destination of each result (no extra moves).
+// q = bit(K0) << 1 | bit(K1); P: 0 none, 1 CNOT K0->K1, 2 CNOT K1->K0, 3 SWAP.
+template <int K0, int K1, int F0, int F1, int P>
+__device__ __forceinline__ void reg_pair(double2 (&a)[16], double x0, double x1) {
+    constexpr int perm[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 3, 2, 1}, {0, 2, 1, 3}};
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
+        const int i[4] = {e, e | (1 << K1), e | (1 << K0), e | (1 << K0) | (1 << K1)};
+        double2 v[4] = {a[i[0]], a[i[1]], a[i[2]], a[i[3]]};
+        rot_s<F1>(v[0], v[1], x1);
+        rot_s<F1>(v[2], v[3], x1);
+        rot_s<F0>(v[0], v[2], x0);
+        rot_s<F0>(v[1], v[3], x0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[i[perm[P][q]]] = v[q];
+    }
+}
+
+template <int K0, int K1>
+__device__ __forceinline__ void reg_pair_dispatch(double2 (&a)[16], int code, double x0,
+                                                  double x1) {
+    switch (code) {  // forms (bits 0-1) and permutation (bits 2-3)
+#define LQ_PAIR_CASE(C) \
+    case C: reg_pair<K0, K1, ((C) & 1), (((C) >> 1) & 1), ((C) >> 2)>(a, x0, x1); break;
+    LQ_PAIR_CASE(0) LQ_PAIR_CASE(1) LQ_PAIR_CASE(2) LQ_PAIR_CASE(3)
+    LQ_PAIR_CASE(4) LQ_PAIR_CASE(5) LQ_PAIR_CASE(6) LQ_PAIR_CASE(7)
+    LQ_PAIR_CASE(8) LQ_PAIR_CASE(9) LQ_PAIR_CASE(10) LQ_PAIR_CASE(11)
+    LQ_PAIR_CASE(12) LQ_PAIR_CASE(13) LQ_PAIR_CASE(14)
+    default: reg_pair<K0, K1, 1, 1, 3>(a, x0, x1); break;
+#undef LQ_PAIR_CASE
+    }
+}
+
 // Diagonal over the register bits: one complex factor per register element,
 // the product of every diagonal gate of the run (computed on the host).
 __device__ __forceinline__ void reg_dtab(double2 (&a)[16], const double *__restrict__ c) {
@@ -349,6 +399,16 @@ __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &
                 }
             } else if (op.type == F_DTAB) {
                 reg_dtab(a, cfull);
+            } else if (op.type == F_PAIR) {
+                const double x0 = c8[0], x1 = c8[1];
+                switch (op.k0 * 4 + op.k1) {
+                case 1: reg_pair_dispatch<0, 1>(a, op.cm, x0, x1); break;
+                case 2: reg_pair_dispatch<0, 2>(a, op.cm, x0, x1); break;
+                case 3: reg_pair_dispatch<0, 3>(a, op.cm, x0, x1); break;
+                case 6: reg_pair_dispatch<1, 2>(a, op.cm, x0, x1); break;
+                case 7: reg_pair_dispatch<1, 3>(a, op.cm, x0, x1); break;
+                default: reg_pair_dispatch<2, 3>(a, op.cm, x0, x1); break;
+                }
             } else if (op.type == F_R1S) {
                 const double x = c8[0];
                 switch (op.k0 * 2 + op.k1) {

@@ -33,6 +33,13 @@ struct GateOp {
     // or [[x, -1], [1, x]] (form 1) with x = m[0]; m[] holds the full real 2x2.
     bool srot = false;
     int sform = 0;
+    // pairrot: an OP_M2 (real4) that is P (R'_b0 (x) R'_b1), R' scaled rotations
+    // with parameters px and forms pf as above, P = pperm: 0 none, 1 CNOT
+    // b0 -> b1, 2 CNOT b1 -> b0, 3 SWAP.  m[] holds the full real 4x4.
+    bool pairrot = false;
+    double px[2] = {0.0, 0.0};
+    int pf[2] = {0, 0};
+    int pperm = 0;
     double m[32] = {0};          // M1: 8 doubles; M2: 32; DIAG: ph[0..3] as 8 doubles
 };
 

@@ -21,7 +21,8 @@ OP_DT = np.dtype([("type", np.int32), ("k0", np.int32), ("k1", np.int32), ("cm",
                   ("param", np.int32), ("coef_alt", np.int32), ("param2", np.int32),
                   ("coef_alt2", np.int32)], align=True)
 
-F_M1, F_M1C, F_X, F_XC, F_DIAG, F_SWAP, F_M2, F_BLOCK3, F_BLOCK4, F_M2R, F_DTAB, F_R1S = range(12)
+(F_M1, F_M1C, F_X, F_XC, F_DIAG, F_SWAP, F_M2, F_BLOCK3, F_BLOCK4, F_M2R, F_DTAB, F_R1S,
+ F_PAIR) = range(13)
 
 
 def dump(n, gates, theta=None):
@@ -172,6 +173,25 @@ def apply_op(a, op, coef, gbase, gp):
                 n0, n1 = x * a0 - a1, a0 + x * a1
             a[e] = np.where(act, n0, a0)
             a[e | (1 << k0)] = np.where(act, n1, a1)
+    elif t == F_PAIR:
+        def rot(y0, y1, x, form):
+            if form == 0:
+                return y0 - x * y1, y1 + x * y0
+            return x * y0 - y1, y0 + x * y1
+        f0, f1, perm = cm & 1, (cm >> 1) & 1, cm >> 2
+        P = [[0, 1, 2, 3], [0, 1, 3, 2], [0, 3, 2, 1], [0, 2, 1, 3]][perm]
+        for e in range(16):
+            if (e & (1 << k0)) or (e & (1 << k1)):
+                continue
+            idx = [e, e | (1 << k1), e | (1 << k0), e | (1 << k0) | (1 << k1)]
+            v = [a[i] for i in idx]
+            v[0], v[1] = rot(v[0], v[1], c[1], f1)
+            v[2], v[3] = rot(v[2], v[3], c[1], f1)
+            v[0], v[2] = rot(v[0], v[2], c[0], f0)
+            v[1], v[3] = rot(v[1], v[3], c[0], f0)
+            old = [a[i] for i in idx]
+            for q in range(4):
+                a[idx[P[q]]] = np.where(act, v[q], old[P[q]])
     elif t == F_DTAB:
         for e in range(16):
             a[e] = np.where(act, a[e] * cpx(e), a[e])

@@ -79,8 +79,11 @@ def test_pair_fold_emits_4x4_ops_and_matches_oracle(kind):
     _, _, _, ops, _ = fe.dump(n, g)
     real = kind in (abi.CNOT, abi.CZ, abi.CPHASE, abi.SWAP, abi.RZZ)
     if real:
-        # two scaled rotations per pair, their scales and phases in tables
-        assert (ops["type"] == fe.F_R1S).sum() == 2 * (n // 2)
+        # one real pair op (two scaled rotations and the permutation) per pair,
+        # the rotations' scales and the Euler phases in diagonal tables
+        pr = ops[ops["type"] == fe.F_PAIR]
+        assert len(pr) == n // 2
+        assert (pr["k0"] < pr["k1"]).all()
         assert (ops["type"] == fe.F_DTAB).any()
         assert not (ops["type"] == fe.F_M2).any()
     else:
