@@ -1148,36 +1148,40 @@ static int launch_pass(lq_state *s, int T, int h, const FusedRound *d_rounds, in
     return LQ_OK;
 }
 
-// Encode the ops of one register round.  Diagonals whose bits are all
-// register bits of the round move as early as they commute and each run of them
-// becomes one F_DTAB: a 16-entry table over the register elements, the product
-// of the run's phases, computed on the host.  A run still open at the end of
-// the round is carried into the next round of the pass (`carry`) when its bits
-// are register bits there too, so it joins that round's first table.
+// Encode the ops of one register round.  Diagonal gates move as early as they
+// commute and each run of them becomes one F_DTAB: a phase table over the
+// round's 16 register elements, the product of the run's phases, computed on
+// the host.  A diagonal bit outside the register set is constant per thread
+// (a thread bit of the tile, or a bit outside the window, constant per tile),
+// so a table may depend on up to two such bits: one 16-entry variant per value.
+// A run still open at the end of the round is carried into the next fused
+// round (`carry`; `has_next` tells whether one follows with no standalone gate
+// in between), where it joins that round's first table.
 static void encode_round(const std::vector<GateOp> &gops, const std::vector<int> &pass_gates,
-                         const PlannedRound &rd, const int *next_rpos, int h, int T,
+                         const PlannedRound &rd, bool has_next, int h, int T,
                          std::vector<const GateOp *> &carry, std::vector<FusedOp> &fops,
                          std::vector<double> &coef, int &mode) {
     using cd = std::complex<double>;
     const int m = T - 4;
-    auto reg_in = [&](const int *rpos, int b) {
+    auto reg = [&](int b) {
         if (!(b < 4 || (b >= h && b < h + m))) return -1;
         const int lp = local_pos(b, h);
         for (int k = 0; k < 4; ++k)
-            if (rpos[k] == lp) return k;
+            if (rd.rpos[k] == lp) return k;
         return -1;
     };
-    auto reg = [&](int b) { return reg_in(rd.rpos, b); };
     const bool merge = real_fold_enabled();
-    auto table_in = [&](const int *rpos, const GateOp &g) {
-        if (!merge || g.type != OP_DIAG || g.renorm) return false;
+    auto outside = [&](const GateOp &g) {  // its non-register bits, as a mask
+        uint64_t o = 0;
         for (int k = 0; k < g.npat; ++k)
-            if (reg_in(rpos, g.pat[k]) < 0) return false;
+            if (reg(g.pat[k]) < 0) o |= 1ull << g.pat[k];
         for (int k = 0; k < g.nfix; ++k)
-            if (reg_in(rpos, g.fix[k]) < 0) return false;
-        return true;
+            if (reg(g.fix[k]) < 0) o |= 1ull << g.fix[k];
+        return o;
     };
-    auto table_ok = [&](const GateOp &g) { return table_in(rd.rpos, g); };
+    auto table_ok = [&](const GateOp &g) {
+        return merge && g.type == OP_DIAG && !g.renorm && popc(outside(g)) <= 2;
+    };
     std::vector<const GateOp *> L(carry.begin(), carry.end());
     carry.clear();
     for (int k : rd.ops) {
@@ -1190,39 +1194,51 @@ static void encode_round(const std::vector<GateOp> &gops, const std::vector<int>
         L.insert(L.begin() + pos, &g);
     }
     std::vector<const GateOp *> pending;
-    uint64_t pbits = 0;
+    uint64_t pbits = 0, pout = 0;
     auto flush = [&]() {
         if (pending.empty()) return;
-        cd tab[16];
-        for (int e = 0; e < 16; ++e) tab[e] = 1.0;
-        for (const GateOp *g : pending)
-            for (int e = 0; e < 16; ++e) {
-                bool on = true;
-                for (int k = 0; k < g->nfix; ++k) on = on && ((e >> reg(g->fix[k])) & 1);
-                if (!on) continue;
-                int pidx = 0;
-                for (int k = 0; k < g->npat; ++k) pidx |= ((e >> reg(g->pat[k])) & 1) << k;
-                tab[e] *= cd(g->m[2 * pidx], g->m[2 * pidx + 1]);
-            }
+        int vb[2] = {-1, -1}, nv = 0;
+        for (int b = 0; b < 64; ++b)
+            if (pout >> b & 1) vb[nv++] = b;
+        auto bitval = [&](int b, int e, int v) {
+            const int k = reg(b);
+            if (k >= 0) return (e >> k) & 1;
+            return b == vb[0] ? v & 1 : (v >> 1) & 1;
+        };
         FusedOp f{};
         f.type = F_DTAB;
         f.coef = (int)coef.size();
-        f.pb0 = f.pb1 = -1;
+        f.npat = nv;
+        f.pb0 = vb[0];
+        f.pb1 = vb[1];
         f.param = f.param2 = -1;
         f.coef_alt = f.coef_alt2 = -1;
-        for (int e = 0; e < 16; ++e) {
-            coef.push_back(tab[e].real());
-            coef.push_back(tab[e].imag());
-        }
+        for (int v = 0; v < (1 << nv); ++v)
+            for (int e = 0; e < 16; ++e) {
+                cd t = 1.0;
+                for (const GateOp *g : pending) {
+                    bool on = true;
+                    for (int k = 0; k < g->nfix; ++k) on = on && bitval(g->fix[k], e, v);
+                    if (!on) continue;
+                    int pidx = 0;
+                    for (int k = 0; k < g->npat; ++k) pidx |= bitval(g->pat[k], e, v) << k;
+                    t *= cd(g->m[2 * pidx], g->m[2 * pidx + 1]);
+                }
+                coef.push_back(t.real());
+                coef.push_back(t.imag());
+            }
         fops.push_back(f);
         mode = std::max(mode, 1);
         pending.clear();
-        pbits = 0;
+        pbits = pout = 0;
     };
     for (const GateOp *g : L) {
         if (table_ok(*g)) {
+            const uint64_t o = outside(*g);
+            if (popc(pout | o) > 2) flush();
             pending.push_back(g);
             pbits |= op_bits(*g);
+            pout |= o;
             continue;
         }
         if (op_bits(*g) & pbits) flush();
@@ -1231,9 +1247,7 @@ static void encode_round(const std::vector<GateOp> &gops, const std::vector<int>
         if (t == F_M2 || t == F_M2R || t == F_R1S || t == F_PAIR) mode = std::max(mode, 1);
         if (t == F_BLOCK3 || t == F_BLOCK4) mode = 2;
     }
-    bool keep = next_rpos != nullptr && !pending.empty();
-    for (const GateOp *g : pending) keep = keep && table_in(next_rpos, *g);
-    if (keep)
+    if (has_next && !pending.empty())
         carry = pending;
     else
         flush();
@@ -1243,17 +1257,23 @@ static void encode_round(const std::vector<GateOp> &gops, const std::vector<int>
 static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<GateOp> &gops,
                          int T, std::vector<FusedRound> &rounds, std::vector<FusedOp> &fops,
                          std::vector<double> &coef, std::vector<PassLaunch> &launches) {
-    for (auto &st : steps) {
+    // diagonal runs carried forward, across rounds and into the next pass when
+    // no standalone gate comes between
+    std::vector<const GateOp *> carry;
+    for (size_t si = 0; si < steps.size(); ++si) {
+        const PlanStep &st = steps[si];
         if (!st.fused) continue;
+        const bool next_pass = si + 1 < steps.size() && steps[si + 1].fused &&
+                               !steps[si + 1].pass.rounds.empty();
         PassLaunch pl{st.pass.h, (int)rounds.size(), (int)st.pass.rounds.size(), 0};
-        std::vector<const GateOp *> carry;
         for (size_t ri = 0; ri < st.pass.rounds.size(); ++ri) {
             const PlannedRound &rd = st.pass.rounds[ri];
-            const int *next = ri + 1 < st.pass.rounds.size() ? st.pass.rounds[ri + 1].rpos : nullptr;
+            const bool has_next = ri + 1 < st.pass.rounds.size() || next_pass;
             FusedRound fr{};
             fill_round(fr, rd.rpos, T, st.pass.h);
             fr.op_begin = (int)fops.size();
-            encode_round(gops, st.pass.gates, rd, next, st.pass.h, T, carry, fops, coef, pl.mode);
+            encode_round(gops, st.pass.gates, rd, has_next, st.pass.h, T, carry, fops, coef,
+                         pl.mode);
             fr.op_end = (int)fops.size();
             rounds.push_back(fr);
         }

@@ -24,7 +24,9 @@ enum FusedOpType {
     F_BLOCK3 = 7, // 8x8 on reg bits 0..2 (matrix bit j <-> reg bit j)
     F_BLOCK4 = 8, // 16x16 on reg bits 0..3
     F_M2R = 9,    // real 4x4 (16 doubles), index = bit(k0)<<1 | bit(k1), k0 < k1
-    F_DTAB = 10,  // amplitude e *= table[e] (16 complex), e = register element index
+    F_DTAB = 10,  // amplitude e *= table[v][e] (16 complex per variant), e = register
+                  // element index, v = values of the npat (<= 2) non-register global
+                  // bits pb0 (lsb), pb1 of the thread's base index
     F_R1S = 11,   // scaled real rotation on reg bit k0, x = coef[0]:
                   // k1 = 0: [[1, -x], [x, 1]];  k1 = 1: [[x, -1], [1, x]]
     F_PAIR = 12   // scaled rotations on reg bits k1 (x = coef[1], form cm bit 1) and
@@ -398,7 +400,11 @@ __device__ __forceinline__ void apply_fused_op(double2 (&a)[16], const FusedOp &
                 default: reg_m2r<2, 3>(a, cfull); break;
                 }
             } else if (op.type == F_DTAB) {
-                reg_dtab(a, cfull);
+                // up to two non-register bits select one of the table's variants
+                int v = 0;
+                if (op.npat > 0) v = (int)((gbase >> op.pb0) & 1ull);
+                if (op.npat > 1) v |= (int)((gbase >> op.pb1) & 1ull) << 1;
+                reg_dtab(a, cfull + 32 * v);
             } else if (op.type == F_PAIR) {
                 const double x0 = c8[0], x1 = c8[1];
                 switch (op.k0 * 4 + op.k1) {

@@ -193,7 +193,14 @@ def apply_op(a, op, coef, gbase, gp):
             for q in range(4):
                 a[idx[P[q]]] = np.where(act, v[q], old[P[q]])
     elif t == F_DTAB:
+        npat, pb0, pb1 = int(op["npat"]), int(op["pb0"]), int(op["pb1"])
+        v = np.zeros_like(gbase)
+        if npat > 0:
+            v = (gbase >> pb0) & 1
+        if npat > 1:
+            v = v | (((gbase >> pb1) & 1) << 1)
+        tab = np.array([cpx(k) for k in range(16 << npat)]).reshape(1 << npat, 16)
         for e in range(16):
-            a[e] = np.where(act, a[e] * cpx(e), a[e])
+            a[e] = np.where(act, a[e] * tab[v, e], a[e])
     else:
         raise NotImplementedError(t)
