@@ -1,11 +1,14 @@
 """GPU: precision form (complex64 state, 5-qubit blocks on tcgen05 with 3xTF32)
 against the complex128 engine on the same circuit.
 
-Tolerances (3xTF32 with FP32 accumulation and complex64 storage is FP32-class
-arithmetic): one block must agree to 1e-5 relative (plain TF32 would give
-~1e-3); whole circuits to per-amplitude max-abs 2e-6 (amplitudes are
-O(2^-n/2)) and fidelity 1 - 1e-4 (FP32 rounding shrinks the norm by ~1e-7 per
-block)."""
+Bars, relative to the state's RMS amplitude (amplitudes are O(2^-n/2), so an
+absolute bar would be loose for large n): one block 1e-5 of the largest
+amplitude (plain TF32 products give ~1e-3: tests/test_tc_split_emulation.py);
+whole circuits max-abs 1e-5 x RMS, |1 - fidelity| 1e-9 and the FP64 norm of
+the input kept to 1e-8.  Measured on a B200: 1.1-5.8e-6 x RMS (12-20 qubits,
+up to 20 layers), norm within 1e-10 -- the tensor cores' FP32 accumulation
+shrinks the state by ~6e-7 per block, which the engine removes by restoring
+the input's FP64 norm after the circuit."""
 import ctypes as C
 
 import numpy as np
@@ -59,11 +62,12 @@ def test_tc_brickwork_matches_complex128(n, layers):
     want = run_c128(n, g)
     got, norm, nb, npass = run_tc(n, g)
     assert nb > 0 and npass > 0
-    err = np.abs(got - want).max()
+    rms = np.sqrt(np.mean(np.abs(want) ** 2))
+    err = np.abs(got - want).max() / rms
     fid = abs(np.vdot(want, got)) ** 2
-    assert err < 2e-6, err
-    assert abs(fid - 1) < 1e-4, fid
-    assert abs(norm - 1) < 1e-4
+    assert err < 1e-5, err
+    assert abs(fid - 1) < 1e-9, fid
+    assert abs(norm - 1) < 1e-8, norm
 
 
 def test_tc_qft_random_state():
@@ -72,8 +76,10 @@ def test_tc_qft_random_state():
     g = workloads.qft_gates(n)
     want = run_c128(n, g, v)
     got, norm, _, _ = run_tc(n, g, v)
-    assert np.abs(got - want).max() < 2e-6
-    assert abs(abs(np.vdot(want, got)) ** 2 - 1) < 1e-4
+    rms = np.sqrt(np.mean(np.abs(want) ** 2))
+    assert np.abs(got - want).max() / rms < 1e-5
+    assert abs(abs(np.vdot(want, got)) ** 2 - 1) < 1e-9
+    assert abs(norm - 1) < 1e-8
 
 
 def test_tc_rejects_complex128_state():
