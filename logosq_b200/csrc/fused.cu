@@ -33,6 +33,7 @@
 #include <mutex>
 
 #include "fused_plan.h"
+#include "fused_round.cuh"
 
 namespace lq {
 
@@ -129,141 +130,81 @@ __global__ void __maxnreg__(168)
     fused_pass_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
 }
 
-// ---------------------------------------------------------------------------
-// Persistent form: one CTA per resident slot walks tiles blockIdx.x,
-// blockIdx.x + G, ... with two tile buffers, so the TMA load of the next tile
-// and the store of the previous one overlap the register rounds of the current
-// one.  The pass program (rounds, ops, coefficients: a few KB) is copied once
-// per CTA into shared memory, so every descriptor and coefficient read in the
-// round loop is a uniform shared-memory broadcast instead of a global load.
-//
-// Program blob layout (16-byte aligned, built by encode_steps):
-//   PassHdr, FusedRound[nrounds], FusedOp[nops], double coef[ncoef]
-// ---------------------------------------------------------------------------
-struct PassHdr {
-    int32_t nrounds, nops, ncoef, bytes;  // bytes: whole blob, multiple of 16
-};
-static_assert(sizeof(PassHdr) == 16, "blob header");
-static_assert(sizeof(FusedRound) % 16 == 0 && sizeof(FusedOp) % 16 == 0, "blob alignment");
-
-__device__ __forceinline__ void tma_load_tile(const CUtensorMap &tmap, uint32_t dst,
-                                              uint32_t bar, uint32_t bytes, int32_t c2,
-                                              int32_t c4) {
-    const int32_t zero = 0;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                 "r"(bytes)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
-        "l"((uint64_t)&tmap), "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(bar)
-        : "memory");
-}
-
+// Ping-pong register rounds (fused_round.cuh) over compact PassOp records;
+// one CTA per tile, as k_fused_pass_narrow.
 template <int MODE>
-__device__ __forceinline__ void fused_persistent_body(const CUtensorMap &tmap, int T,
-                                                      TileCoords tc,
-                                                      const unsigned char *__restrict__ prog,
-                                                      unsigned *__restrict__ flag) {
+__device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, TileCoords tc,
+                                              const FusedRound *__restrict__ rounds, int nrounds,
+                                              const PassOp *__restrict__ ops,
+                                              const double *__restrict__ coef,
+                                              unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t tile_bytes = 16u << T;
-    uint64_t *bar = (uint64_t *)(base + 2 * tile_bytes);
-    unsigned char *pr = base + 2 * tile_bytes + 64;
-    // buffer b at buf0 + b * tile_bytes, its barrier at bar0 + 8 * b
-    const uint32_t buf0 = smem_u32(base), bar0 = smem_u32(bar);
+    uint64_t *bar = (uint64_t *)(base + tile_bytes);
+    const uint32_t tile_a = smem_u32(base);
+    const uint32_t bar_a = smem_u32(bar);
     const int tid = threadIdx.x;
-    const int G = gridDim.x;
-    const int ntiles = tc.ntiles;
-    const int lo_mask = (1 << (tc.h - 4)) - 1;
-
-    // Stage the pass program.
-    const int pbytes = reinterpret_cast<const PassHdr *>(prog)->bytes;
-    for (int i = tid; i < pbytes / 16; i += blockDim.x)
-        reinterpret_cast<int4 *>(pr)[i] = reinterpret_cast<const int4 *>(prog)[i];
+    const int32_t zero = 0;
+    const int tile = blockIdx.x;
+    const int32_t c2 = tile & ((1 << (tc.h - 4)) - 1), c4 = tile >> (tc.h - 4);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const PassHdr hdr = *reinterpret_cast<const PassHdr *>(pr);
-    const FusedRound *rounds = reinterpret_cast<const FusedRound *>(pr + sizeof(PassHdr));
-    const FusedOp *ops = reinterpret_cast<const FusedOp *>(rounds + hdr.nrounds);
-    const double *coef = reinterpret_cast<const double *>(ops + hdr.nops);
-    auto coef_of = [&](const FusedOp &op) { return coef + op.coef; };
-
     if (tid == 0) {
-        for (int b = 0; b < 2; ++b) {
-            const int t = blockIdx.x + b * G;
-            if (t < ntiles)
-                tma_load_tile(tmap, buf0 + b * tile_bytes, bar0 + 8 * b, tile_bytes, t & lo_mask,
-                              t >> (tc.h - 4));
-        }
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
+                     "r"(tile_bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(tile_a),
+            "l"((uint64_t)&tmap), "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(bar_a)
+            : "memory");
     }
-    int k = 0;
-    for (int t = blockIdx.x; t < ntiles; t += G, ++k) {
-        const int b = k & 1;
-        const uint32_t buf = buf0 + b * tile_bytes, bb = bar0 + 8 * b;
-        const bool ok = mbar_wait(bb, (k >> 1) & 1);
-        if (__syncthreads_or(!ok)) {
-            // A load did not complete within the bound: report, then wait (bounded) for
-            // every load still in flight into this CTA's buffers before leaving.
-            if (tid == 0) {
-                atomicOr(flag, kFlagTimeout);
-                mbar_wait(bb, (k >> 1) & 1);
-                if (t + G < ntiles) mbar_wait(bar0 + 8 * (b ^ 1), ((k + 1) >> 1) & 1);
-            }
-            break;
-        }
-        const int32_t c2 = t & lo_mask, c4 = t >> (tc.h - 4);
-        const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
-        for (int r = 0; r < hdr.nrounds; ++r) {
-            run_round<MODE>(buf, rounds[r], ops, coef_of, tile_base, tc.h, tid);
-            __syncthreads();
-        }
-        // Make the generic-proxy writes visible to the TMA engine, then store.
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+    if (!mbar_wait(bar_a, 0)) {
+        // leave only once the load no longer targets this CTA's shared memory
         if (tid == 0) {
-            const int32_t zero = 0;
-            asm volatile(
-                "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
-                " [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"((uint64_t)&tmap),
-                "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(buf)
-                : "memory");
-            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-            const int tn = t + 2 * G;
-            if (tn < ntiles) {
-                // the buffer is reloaded once the store has read it
-                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-                tma_load_tile(tmap, buf, bb, tile_bytes, tn & lo_mask, tn >> (tc.h - 4));
-            }
+            atomicOr(flag, kFlagTimeout);
+            mbar_wait(bar_a, 0);
         }
+        return;
     }
-    // Shared memory must stay allocated until the last store has read it.
-    if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
+    for (int r = 0; r < nrounds; ++r) {
+        run_round_pp<MODE>(tile_a, rounds[r], ops, coef, tile_base, tc.h, tid);
+        __syncthreads();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+        asm volatile(
+            "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
+            " [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"((uint64_t)&tmap),
+            "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(tile_a)
+            : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        // shared memory is released when the CTA exits: the store must have read it
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256, 1)
-    k_fused_persist(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
-                    const unsigned char *__restrict__ prog, unsigned *__restrict__ flag) {
-    fused_persistent_body<MODE>(tmap, T, tc, prog, flag);
+    k_fused_pp(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
+               const FusedRound *__restrict__ rounds, int nrounds, const PassOp *__restrict__ ops,
+               const double *__restrict__ coef, unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
 }
 
 template <int MODE>
-__global__ void __maxnreg__(168)
-    k_fused_persist_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
-                           const unsigned char *__restrict__ prog, unsigned *__restrict__ flag) {
-    fused_persistent_body<MODE>(tmap, T, tc, prog, flag);
-}
-
-template <int MODE>
-__global__ void __maxnreg__(192)
-    k_fused_persist_narrow192(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
-                           const unsigned char *__restrict__ prog, unsigned *__restrict__ flag) {
-    fused_persistent_body<MODE>(tmap, T, tc, prog, flag);
+__global__ void __maxnreg__(232)
+    k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
+                      const FusedRound *__restrict__ rounds, int nrounds,
+                      const PassOp *__restrict__ ops, const double *__restrict__ coef,
+                      unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -543,13 +484,15 @@ static bool monomial4(const std::complex<double> G[16], int p[4], std::complex<d
 // Scaled rotation op on bit b: R = [[c, -s], [s, c]] = sigma * R' with R' one
 // FMA per component (form 0: c >= s, x = s/c, sigma = c; form 1: x = c/s,
 // sigma = s).
+constexpr double kMinScaledCos = 1e-3;
+
 static GateOp scaled_rotation(int b, double c, double s, double &sigma) {
     GateOp g{};
     g.type = OP_M1;
     g.t = b;
     g.srot = true;
     double r[4];
-    if (c >= s) {
+    if (c >= kMinScaledCos) {  // x = s / c <= 1000: still one FMA per component
         const double x = s / c;
         g.sform = 0;
         sigma = c;
@@ -596,7 +539,8 @@ static bool real_fold(const std::complex<double> G[16], const std::complex<doubl
     const int pc = p[0] | p[1] << 2 | p[2] << 4 | p[3] << 6;
     const int P_ID = 0 | 1 << 2 | 2 << 4 | 3 << 6, P_CX = 0 | 1 << 2 | 3 << 4 | 2 << 6,
               P_XC = 0 | 3 << 2 | 2 << 4 | 1 << 6, P_SW = 0 | 2 << 2 | 1 << 4 | 3 << 6;
-    if (real_fold_mode() >= 2 && (pc == P_ID || pc == P_CX || pc == P_XC || pc == P_SW)) {
+    if (real_fold_mode() >= 2 && (pc == P_ID || pc == P_CX || pc == P_XC || pc == P_SW) &&
+        ex.c >= kMinScaledCos && ey.c >= kMinScaledCos) {
         double sx, sy;
         const GateOp rxo = scaled_rotation(bx, ex.c, ex.s, sx);
         const GateOp ryo = scaled_rotation(by, ey.c, ey.s, sy);
@@ -1000,123 +944,80 @@ static int set_smem_attrs() {
     return LQ_OK;
 }
 
-static bool legacy_kernel() {
+static int pp_engine() {  // 1: ping-pong register rounds over PassOp records
     static const int v = [] {
-        const char *e = getenv("LQ_FUSED_PERSIST");
+        const char *e = getenv("LQ_FUSED_ENGINE");
         return e ? atoi(e) : 0;
     }();
-    return v == 0;
+    return v;
 }
 
-constexpr int kMaxPersistSmem = 227 * 1024;
-
-static size_t persist_smem(int T, int blob_bytes) {
-    return 1024 + 2 * (16u << T) + 64 + (size_t)blob_bytes;
+static int pair_index(int a, int b) {
+    if (a > b) std::swap(a, b);
+    static const int idx[4][4] = {{-1, 0, 1, 2}, {0, -1, 3, 4}, {1, 3, -1, 5}, {2, 4, 5, -1}};
+    return idx[a][b];
 }
 
-static int set_persist_attrs() {
+// The kernel record of one encoded op (flat dispatch code, see PassCode).
+static PassOp pass_op(const FusedOp &f) {
+    PassOp p{};
+    p.coef = f.coef;
+    p.cm = f.cm;
+    p.gmask = f.gmask;
+    p.fixmask = f.fixmask;
+    auto packbits = [](int pb0, int pb1, int npat) {
+        return (pb0 < 0 ? 0 : pb0) | (pb1 < 0 ? 0 : pb1) << 8 | npat << 16;
+    };
+    switch (f.type) {
+    case F_M1: p.code = PC_M1 + f.k0; break;
+    case F_M1C: p.code = PC_M1C + f.k0; break;
+    case F_X: p.code = PC_X + f.k0; break;
+    case F_XC: p.code = PC_XC + f.k0; break;
+    case F_DIAG: p.code = PC_DIAG; p.bits = packbits(f.pb0, f.pb1, f.npat); break;
+    case F_SWAP: p.code = PC_SWAP + pair_index(f.k0, f.k1); break;
+    case F_M2: p.code = PC_M2 + pair_index(f.k0, f.k1); break;
+    case F_M2R: p.code = PC_M2R + pair_index(f.k0, f.k1); break;
+    case F_DTAB: p.code = PC_DTAB; p.bits = packbits(f.pb0, f.pb1, f.npat); break;
+    case F_PAIR: p.code = PC_PAIR + pair_index(f.k0, f.k1) * 4 + (f.cm >> 2); p.cm = 0; break;
+    case F_BLOCK3: p.code = PC_BLOCK3; break;
+    default: p.code = PC_BLOCK4; break;
+    }
+    return p;
+}
+
+static int set_pp_attrs() {
     static bool done = false;
     if (done) return LQ_OK;
-#define LQ_ATTR(K) \
-    LQ_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPersistSmem))
-    LQ_ATTR(k_fused_persist<0>);
-    LQ_ATTR(k_fused_persist<1>);
-    LQ_ATTR(k_fused_persist<2>);
-    LQ_ATTR(k_fused_persist_narrow<0>);
-    LQ_ATTR(k_fused_persist_narrow<1>);
-    LQ_ATTR(k_fused_persist_narrow<2>);
-    LQ_ATTR(k_fused_persist_narrow192<0>);
-    LQ_ATTR(k_fused_persist_narrow192<1>);
-    LQ_ATTR(k_fused_persist_narrow192<2>);
+    const int mx = (int)fused_smem(kMaxT);
+#define LQ_ATTR(K) LQ_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
+    LQ_ATTR(k_fused_pp<1>);
+    LQ_ATTR(k_fused_pp_narrow<1>);
 #undef LQ_ATTR
     done = true;
     return LQ_OK;
 }
 
-static int num_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            sms <= 0)
-            sms = 148;
-    }
-    return sms;
-}
-
-// One fused pass with the persistent kernel; blob = the pass program in device
-// memory (PassHdr layout), blob_bytes its size.
-static int launch_pass_persist(lq_state *s, int T, int h, const unsigned char *d_blob,
-                               int blob_bytes, int mode) {
+static int launch_pass_pp(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
+                          const PassOp *d_ops, const double *d_coef, int mode) {
     const int n = s->n;
     const int m = T - 4;
     CUtensorMap map;
     LQ_TRY(make_tile_map(&map, s->d, n, h, m));
     const int ntiles = 1 << (n - T);
     TileCoords tc{h, h + m, ntiles};
-    const size_t smem = persist_smem(T, blob_bytes);
-    if (smem > (size_t)kMaxPersistSmem)
-        return set_error(LQ_ERR_UNSUPPORTED, "fused pass program too large (%d bytes)",
-                         blob_bytes);
-    LQ_TRY(set_persist_attrs());
-    const int threads = 1 << (T - 4);
-    const void *fn;
-    if (T >= 12)
-        fn = mode == 2 ? (const void *)k_fused_persist<2>
-             : mode == 1 ? (const void *)k_fused_persist<1> : (const void *)k_fused_persist<0>;
-    else if (getenv("LQ_FUSED_REGS") && atoi(getenv("LQ_FUSED_REGS")) == 192)
-        fn = mode == 2 ? (const void *)k_fused_persist_narrow192<2>
-             : mode == 1 ? (const void *)k_fused_persist_narrow192<1>
-                         : (const void *)k_fused_persist_narrow192<0>;
-    else
-        fn = mode == 2 ? (const void *)k_fused_persist_narrow<2>
-             : mode == 1 ? (const void *)k_fused_persist_narrow<1>
-                         : (const void *)k_fused_persist_narrow<0>;
-    int per_sm = 0;
-    LQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
-    if (per_sm < 1) return set_error(LQ_ERR_CUDA, "fused pass kernel does not fit an SM");
-    const int grid = std::min(ntiles, per_sm * num_sms());
+    const size_t smem = fused_smem(T);
+    LQ_TRY(set_pp_attrs());
     prof_begin(s->stream, kProfFused);
-    void *args[] = {(void *)&map, (void *)&T, (void *)&tc, (void *)&d_blob, (void *)&s->d_flag};
-    LQ_CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, s->stream));
+    const dim3 blk(1u << (T - 4));
+#define LQ_FUSED_LAUNCH(K) \
+    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, s->d_flag)
+    (void)mode;  // one op set (4x4, pair and table ops included); blocks use launch_pass
+    if (T >= 12) LQ_FUSED_LAUNCH(k_fused_pp<1>);
+    else LQ_FUSED_LAUNCH(k_fused_pp_narrow<1>);
+#undef LQ_FUSED_LAUNCH
     prof_end(s->stream, kProfFused);
+    LQ_CUDA_TRY(cudaGetLastError());
     return LQ_OK;
-}
-
-// Slice the program of each launch out of the circuit-wide arrays into one
-// blob per pass (op and coefficient indices rebased to the pass).
-static void make_blobs(const std::vector<FusedRound> &rounds, const std::vector<FusedOp> &fops,
-                       const std::vector<double> &coef, int round_begin, int nrounds,
-                       std::vector<unsigned char> &out) {
-    const int o0 = nrounds ? rounds[round_begin].op_begin : 0;
-    const int o1 = nrounds ? rounds[round_begin + nrounds - 1].op_end : 0;
-    const int c0 = o1 > o0 ? fops[o0].coef : 0;
-    const int c1 = o1 > o0 ? (o1 < (int)fops.size() ? fops[o1].coef : (int)coef.size()) : 0;
-    PassHdr hd{nrounds, o1 - o0, c1 - c0, 0};
-    size_t bytes = sizeof(PassHdr) + sizeof(FusedRound) * nrounds + sizeof(FusedOp) * hd.nops +
-                   sizeof(double) * hd.ncoef;
-    bytes = (bytes + 15) / 16 * 16;
-    hd.bytes = (int32_t)bytes;
-    const size_t at = out.size();
-    out.resize(at + bytes, 0);
-    unsigned char *p = out.data() + at;
-    memcpy(p, &hd, sizeof(hd));
-    p += sizeof(hd);
-    for (int r = 0; r < nrounds; ++r) {
-        FusedRound fr = rounds[round_begin + r];
-        fr.op_begin -= o0;
-        fr.op_end -= o0;
-        memcpy(p, &fr, sizeof(fr));
-        p += sizeof(fr);
-    }
-    for (int o = o0; o < o1; ++o) {
-        FusedOp f = fops[o];
-        f.coef -= c0;
-        memcpy(p, &f, sizeof(f));
-        p += sizeof(f);
-    }
-    if (hd.ncoef) memcpy(p, coef.data() + c0, sizeof(double) * hd.ncoef);
 }
 
 static int launch_pass(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
@@ -1308,19 +1209,23 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
     std::vector<double> coef;
     std::vector<PassLaunch> launches;
     encode_steps(steps, gops, T, rounds, fops, coef, launches);
-    if (!legacy_kernel()) {
-        std::vector<unsigned char> blobs;
-        std::vector<size_t> at(launches.size());
-        for (size_t i = 0; i < launches.size(); ++i) {
-            at[i] = blobs.size();
-            make_blobs(rounds, fops, coef, launches[i].round_begin, launches[i].nrounds, blobs);
-        }
-        LQ_TRY(ensure_prog(s, blobs.size() + 256));
+    if (pp_engine() == 1) {
+        std::vector<PassOp> pops(fops.size());
+        for (size_t i = 0; i < fops.size(); ++i) pops[i] = pass_op(fops[i]);
+        const size_t rb = rounds.size() * sizeof(FusedRound);
+        const size_t ob = pops.size() * sizeof(PassOp);
+        const size_t cb = coef.size() * sizeof(double);
+        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+        LQ_TRY(ensure_prog(s, al(rb) + al(ob) + al(cb) + 256));
+        char *dp = (char *)s->d_prog;
+        FusedRound *d_rounds = (FusedRound *)dp;
+        PassOp *d_ops = (PassOp *)(dp + al(rb));
+        double *d_coef = (double *)(dp + al(rb) + al(ob));
         // The program buffer may still be read by a previous call's kernels.
         LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
-        if (!blobs.empty())
-            LQ_CUDA_TRY(cudaMemcpy(s->d_prog, blobs.data(), blobs.size(), cudaMemcpyHostToDevice));
-        const unsigned char *dp = (const unsigned char *)s->d_prog;
+        if (rb) LQ_CUDA_TRY(cudaMemcpy(d_rounds, rounds.data(), rb, cudaMemcpyHostToDevice));
+        if (ob) LQ_CUDA_TRY(cudaMemcpy(d_ops, pops.data(), ob, cudaMemcpyHostToDevice));
+        if (cb) LQ_CUDA_TRY(cudaMemcpy(d_coef, coef.data(), cb, cudaMemcpyHostToDevice));
         size_t li = 0;
         for (auto &st : steps) {
             if (!st.fused) {
@@ -1328,11 +1233,9 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
                 s->last_launches += gops[st.gate].renorm ? 3 : 1;
                 continue;
             }
-            const size_t off = at[li];
-            const int bytes =
-                (int)((li + 1 < at.size() ? at[li + 1] : blobs.size()) - off);
-            LQ_TRY(launch_pass_persist(s, T, launches[li].h, dp + off, bytes, launches[li].mode));
-            ++li;
+            const PassLaunch &pl = launches[li++];
+            LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef,
+                                  pl.mode));
             s->last_launches += 1;
             s->last_passes += 1;
         }
@@ -1408,17 +1311,6 @@ int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m) {
     fo.param = fo.coef_alt = fo.param2 = fo.coef_alt2 = -1;
     fo.coef = 0;
     const size_t cb = sizeof(double) * 2 * (1 << k) * (1 << k);
-    if (!legacy_kernel()) {
-        std::vector<FusedRound> rv{fr};
-        std::vector<FusedOp> ov{fo};
-        std::vector<double> cv(m, m + cb / sizeof(double));
-        std::vector<unsigned char> blob;
-        make_blobs(rv, ov, cv, 0, 1, blob);
-        LQ_TRY(ensure_prog(s, blob.size() + 256));
-        LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
-        LQ_CUDA_TRY(cudaMemcpy(s->d_prog, blob.data(), blob.size(), cudaMemcpyHostToDevice));
-        return launch_pass_persist(s, T, h, (const unsigned char *)s->d_prog, (int)blob.size(), 2);
-    }
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     LQ_TRY(ensure_prog(s, al(sizeof(FusedRound)) + al(sizeof(FusedOp)) + al(cb) + 256));
     char *dp = (char *)s->d_prog;

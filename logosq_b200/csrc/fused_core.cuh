@@ -29,9 +29,9 @@ enum FusedOpType {
                   // bits pb0 (lsb), pb1 of the thread's base index
     F_R1S = 11,   // scaled real rotation on reg bit k0, x = coef[0]:
                   // k1 = 0: [[1, -x], [x, 1]];  k1 = 1: [[x, -1], [1, x]]
-    F_PAIR = 12   // scaled rotations on reg bits k1 (x = coef[1], form cm bit 1) and
-                  // k0 (x = coef[0], form cm bit 0), then a permutation of the pair
-                  // (cm >> 2: 0 none, 1 CNOT k0 -> k1, 2 CNOT k1 -> k0, 3 SWAP)
+    F_PAIR = 12   // scaled rotations [[1, -x], [x, 1]] on reg bits k1 (x = coef[1]) and
+                  // k0 (x = coef[0]), then a permutation of the pair (cm >> 2: 0 none,
+                  // 1 CNOT k0 -> k1, 2 CNOT k1 -> k0, 3 SWAP; cm bits 0-1 are 0)
 };
 
 struct FusedOp {
@@ -245,15 +245,12 @@ __device__ __forceinline__ void reg_pair(double2 (&a)[16], double x0, double x1)
 template <int K0, int K1>
 __device__ __forceinline__ void reg_pair_dispatch(double2 (&a)[16], int code, double x0,
                                                   double x1) {
-    switch (code) {  // forms (bits 0-1) and permutation (bits 2-3)
-#define LQ_PAIR_CASE(C) \
-    case C: reg_pair<K0, K1, ((C) & 1), (((C) >> 1) & 1), ((C) >> 2)>(a, x0, x1); break;
-    LQ_PAIR_CASE(0) LQ_PAIR_CASE(1) LQ_PAIR_CASE(2) LQ_PAIR_CASE(3)
-    LQ_PAIR_CASE(4) LQ_PAIR_CASE(5) LQ_PAIR_CASE(6) LQ_PAIR_CASE(7)
-    LQ_PAIR_CASE(8) LQ_PAIR_CASE(9) LQ_PAIR_CASE(10) LQ_PAIR_CASE(11)
-    LQ_PAIR_CASE(12) LQ_PAIR_CASE(13) LQ_PAIR_CASE(14)
-    default: reg_pair<K0, K1, 1, 1, 3>(a, x0, x1); break;
-#undef LQ_PAIR_CASE
+    // the planner emits both rotations in form 0; code >> 2 is the permutation
+    switch (code >> 2) {
+    case 0: reg_pair<K0, K1, 0, 0, 0>(a, x0, x1); break;
+    case 1: reg_pair<K0, K1, 0, 0, 1>(a, x0, x1); break;
+    case 2: reg_pair<K0, K1, 0, 0, 2>(a, x0, x1); break;
+    default: reg_pair<K0, K1, 0, 0, 3>(a, x0, x1); break;
     }
 }
 
