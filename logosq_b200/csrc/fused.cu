@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(256, 1)
 }
 
 template <int MODE>
-__global__ void __maxnreg__(232)
+__global__ void __maxnreg__(240)
     k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                       const FusedRound *__restrict__ rounds, int nrounds,
                       const PassOp *__restrict__ ops, const double *__restrict__ coef,
@@ -1211,7 +1211,13 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
     encode_steps(steps, gops, T, rounds, fops, coef, launches);
     if (pp_engine() == 1) {
         std::vector<PassOp> pops(fops.size());
-        for (size_t i = 0; i < fops.size(); ++i) pops[i] = pass_op(fops[i]);
+        for (size_t i = 0; i < fops.size(); ++i) {
+            pops[i] = pass_op(fops[i]);
+            if (fops[i].type == F_PAIR) {
+                pops[i].x0 = coef[fops[i].coef];
+                pops[i].x1 = coef[fops[i].coef + 1];
+            }
+        }
         const size_t rb = rounds.size() * sizeof(FusedRound);
         const size_t ob = pops.size() * sizeof(PassOp);
         const size_t cb = coef.size() * sizeof(double);

@@ -25,8 +25,9 @@ struct PassOp {
     int32_t bits;      // DIAG: pb0 | pb1 << 8 | npat << 16; DTAB: variant bits, same packing
     uint64_t gmask;    // thread-level condition: global bits outside R that must be 1
     uint64_t fixmask;  // DIAG: element condition
+    double x0, x1;     // PAIR: the two rotation parameters (no coefficient load)
 };
-static_assert(sizeof(PassOp) == 32, "PassOp layout");
+static_assert(sizeof(PassOp) == 48, "PassOp layout");
 
 // Flat codes.  Register-bit pairs (k0 < k1) are numbered
 // 0:(0,1) 1:(0,2) 2:(0,3) 3:(1,2) 4:(1,3) 5:(2,3).
@@ -280,7 +281,7 @@ __device__ __forceinline__ void pp_apply(const double2 (&s)[16], double2 (&d)[16
         break;
 #define LQ_PR(P, Q)                                                                          \
     case PC_PAIR + P * 4 + Q:                                                                \
-        if constexpr (MODE >= 1) pp_pair<pair_k0(P), pair_k1(P), 0, 0, Q>(s, d, c[0], c[1]); \
+        if constexpr (MODE >= 1) pp_pair<pair_k0(P), pair_k1(P), 0, 0, Q>(s, d, op.x0, op.x1); \
         break;
 #define LQ_PR4(P) LQ_PR(P, 0) LQ_PR(P, 1) LQ_PR(P, 2) LQ_PR(P, 3)
         LQ_PR4(0) LQ_PR4(1) LQ_PR4(2) LQ_PR4(3) LQ_PR4(4) LQ_PR4(5)
@@ -315,9 +316,10 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
     const int o1 = rd.op_end;
     int o = rd.op_begin;
     for (; o + 1 < o1; o += 2) {
+        // both records first: the second load is hidden behind the first op
         const PassOp p0 = ops[o];
-        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
         const PassOp p1 = ops[o + 1];
+        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
         pp_apply<MODE>(b, a, p1, coef + p1.coef, gbase, rd.gpos);
     }
     const bool odd = o < o1;

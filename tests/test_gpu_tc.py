@@ -4,8 +4,10 @@ against the complex128 engine on the same circuit.
 Bars, relative to the state's RMS amplitude (amplitudes are O(2^-n/2), so an
 absolute bar would be loose for large n): one block 1e-5 of the largest
 amplitude (plain TF32 products give ~1e-3: tests/test_tc_split_emulation.py);
-whole circuits max-abs 1e-5 x RMS, |1 - fidelity| 1e-9 and the FP64 norm of
-the input kept to 1e-8.  Measured on a B200: 1.1-5.8e-6 x RMS (12-20 qubits,
+whole circuits max-abs 1e-5 x RMS, |1 - fidelity| 1e-8 and the FP64 norm of
+the input kept to 1e-8 (rounding the restored amplitudes to complex64 moves the
+norm by ~1e-9, so the unnormalised fidelity cannot be held tighter).  Measured
+on a B200: 1.1-5.8e-6 x RMS (12-20 qubits,
 up to 20 layers), norm within 1e-10 -- the tensor cores' FP32 accumulation
 shrinks the state by ~6e-7 per block, which the engine removes by restoring
 the input's FP64 norm after the circuit."""
@@ -66,7 +68,7 @@ def test_tc_brickwork_matches_complex128(n, layers):
     err = np.abs(got - want).max() / rms
     fid = abs(np.vdot(want, got)) ** 2
     assert err < 1e-5, err
-    assert abs(fid - 1) < 1e-9, fid
+    assert abs(fid - 1) < 1e-8, fid
     assert abs(norm - 1) < 1e-8, norm
 
 
@@ -78,7 +80,7 @@ def test_tc_qft_random_state():
     got, norm, _, _ = run_tc(n, g, v)
     rms = np.sqrt(np.mean(np.abs(want) ** 2))
     assert np.abs(got - want).max() / rms < 1e-5
-    assert abs(abs(np.vdot(want, got)) ** 2 - 1) < 1e-9
+    assert abs(abs(np.vdot(want, got)) ** 2 - 1) < 1e-8
     assert abs(norm - 1) < 1e-8
 
 
