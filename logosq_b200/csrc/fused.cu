@@ -198,8 +198,15 @@ __global__ void __launch_bounds__(256, 1)
     fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
 }
 
+// 168 registers: six 64-thread CTAs per SM at tile bits 10.  Measured on a
+// 30-qubit brickwork: 481 ms per step at 168 registers (a few spills outside
+// the hot ops), 540 at 192, 518 at 240 -- resident warps matter more than the
+// last registers.
+#ifndef LQ_PP_MAXNREG
+#define LQ_PP_MAXNREG 168
+#endif
 template <int MODE>
-__global__ void __maxnreg__(240)
+__global__ void __maxnreg__(LQ_PP_MAXNREG)
     k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                       const FusedRound *__restrict__ rounds, int nrounds,
                       const PassOp *__restrict__ ops, const double *__restrict__ coef,
@@ -947,7 +954,7 @@ static int set_smem_attrs() {
 static int pp_engine() {  // 1: ping-pong register rounds over PassOp records
     static const int v = [] {
         const char *e = getenv("LQ_FUSED_ENGINE");
-        return e ? atoi(e) : 0;
+        return e ? atoi(e) : 1;
     }();
     return v;
 }

@@ -187,7 +187,6 @@ __device__ __forceinline__ void pp_dtab(const double2 (&s)[16], double2 (&d)[16]
 __device__ __forceinline__ void pp_diag(const double2 (&s)[16], double2 (&d)[16],
                                         const PassOp &op, const double *__restrict__ c,
                                         uint64_t gbase, const uint64_t *__restrict__ gpp) {
-    const uint64_t gp[4] = {gpp[0], gpp[1], gpp[2], gpp[3]};
     const uint64_t fm = op.fixmask;
     const int npat = (op.bits >> 16) & 0xff;
     const int pb0 = op.bits & 0xff, pb1 = (op.bits >> 8) & 0xff;
@@ -196,8 +195,8 @@ __device__ __forceinline__ void pp_diag(const double2 (&s)[16], double2 (&d)[16]
                            make_double2(c[4], c[5]), make_double2(c[6], c[7])};
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-        const uint64_t gi = gbase | ((e & 1) ? gp[0] : 0ull) | ((e & 2) ? gp[1] : 0ull) |
-                            ((e & 4) ? gp[2] : 0ull) | ((e & 8) ? gp[3] : 0ull);
+        const uint64_t gi = gbase | ((e & 1) ? gpp[0] : 0ull) | ((e & 2) ? gpp[1] : 0ull) |
+                            ((e & 4) ? gpp[2] : 0ull) | ((e & 8) ? gpp[3] : 0ull);
         const double2 v = s[e];
         if ((gi & fm) != fm) {
             d[e] = v;
@@ -307,20 +306,36 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
     for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
     const uint32_t sb = (uint32_t)swz(tbase) << 4;
     const uint64_t gbase = tile_base | (uint64_t)(tbase & 15) | ((uint64_t)(tbase >> 4) << h);
+    // The swizzle is linear over XOR, so element e's offset is the XOR of the
+    // offsets of its set register bits: four loads instead of sixteen.
+    const uint32_t E0 = (uint32_t)rd.eoff[1], E1 = (uint32_t)rd.eoff[2];
+    const uint32_t E2 = (uint32_t)rd.eoff[4], E3 = (uint32_t)rd.eoff[8];
+    auto addr_of = [&](int e) {
+        const uint32_t x = ((e & 1) ? E0 : 0u) ^ ((e & 2) ? E1 : 0u) ^ ((e & 4) ? E2 : 0u) ^
+                           ((e & 8) ? E3 : 0u);
+        return tile_a + (sb ^ x);
+    };
     double2 a[16], b[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-        const uint32_t addr = tile_a + (sb ^ (uint32_t)rd.eoff[e]);
+        const uint32_t addr = addr_of(e);
         asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(a[e].x), "=d"(a[e].y) : "r"(addr));
     }
     const int o1 = rd.op_end;
     int o = rd.op_begin;
     for (; o + 1 < o1; o += 2) {
+#ifndef LQ_PP_NO_PRELOAD
         // both records first: the second load is hidden behind the first op
         const PassOp p0 = ops[o];
         const PassOp p1 = ops[o + 1];
         pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
         pp_apply<MODE>(b, a, p1, coef + p1.coef, gbase, rd.gpos);
+#else
+        const PassOp p0 = ops[o];
+        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
+        const PassOp p1 = ops[o + 1];
+        pp_apply<MODE>(b, a, p1, coef + p1.coef, gbase, rd.gpos);
+#endif
     }
     const bool odd = o < o1;
     if (odd) {
@@ -329,7 +344,7 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
     }
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-        const uint32_t addr = tile_a + (sb ^ (uint32_t)rd.eoff[e]);
+        const uint32_t addr = addr_of(e);
         const double2 v = odd ? b[e] : a[e];
         asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y)
                      : "memory");
