@@ -1217,13 +1217,31 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
     std::vector<PassLaunch> launches;
     encode_steps(steps, gops, T, rounds, fops, coef, launches);
     if (pp_engine() == 1) {
-        std::vector<PassOp> pops(fops.size());
-        for (size_t i = 0; i < fops.size(); ++i) {
-            pops[i] = pass_op(fops[i]);
-            if (fops[i].type == F_PAIR) {
-                pops[i].x0 = coef[fops[i].coef];
-                pops[i].x1 = coef[fops[i].coef + 1];
+        // Kernel records, round by round: a table followed by a pair op in the
+        // same round becomes one record (PC_TPAIR), so the round dispatches once.
+        std::vector<PassOp> pops;
+        pops.reserve(fops.size());
+        for (auto &fr : rounds) {
+            const int b0 = (int)pops.size();
+            for (int o = fr.op_begin; o < fr.op_end; ++o) {
+                const FusedOp &f = fops[o];
+                PassOp p = pass_op(f);
+                if (f.type == F_PAIR) {
+                    p.x0 = coef[f.coef];
+                    p.x1 = coef[f.coef + 1];
+                }
+                if (f.type == F_DTAB && o + 1 < fr.op_end && fops[o + 1].type == F_PAIR &&
+                    fops[o + 1].gmask == 0 && f.gmask == 0) {
+                    const FusedOp &g = fops[o + 1];
+                    p.code = PC_TPAIR + pair_index(g.k0, g.k1) * 4 + (g.cm >> 2);
+                    p.x0 = coef[g.coef];
+                    p.x1 = coef[g.coef + 1];
+                    ++o;  // the pair is part of this record
+                }
+                pops.push_back(p);
             }
+            fr.op_begin = b0;
+            fr.op_end = (int)pops.size();
         }
         const size_t rb = rounds.size() * sizeof(FusedRound);
         const size_t ob = pops.size() * sizeof(PassOp);

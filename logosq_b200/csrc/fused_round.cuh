@@ -44,7 +44,8 @@ enum PassCode {
     PC_PAIR = 36,    // + pair * 4 + perm (24); both rotations in form 0
     PC_BLOCK3 = 60,
     PC_BLOCK4 = 61,
-    PC_COUNT = 62
+    PC_TPAIR = 62,   // + pair * 4 + perm (24): a diagonal table, then a pair op
+    PC_COUNT = 86
 };
 
 __host__ __device__ constexpr int pair_k0(int p) { return p < 3 ? 0 : p < 5 ? 1 : 2; }
@@ -174,6 +175,33 @@ __device__ __forceinline__ void pp_pair(const double2 (&s)[16], double2 (&d)[16]
     }
 }
 
+// A diagonal table (16 complex factors at c) and then a pair op, in one pass
+// over the registers.
+template <int K0, int K1, int P>
+__device__ __forceinline__ void pp_tpair(const double2 (&s)[16], double2 (&d)[16],
+                                         const double *__restrict__ c, double x0, double x1) {
+    constexpr int perm[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 3, 2, 1}, {0, 2, 1, 3}};
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        if ((e & (1 << K0)) || (e & (1 << K1))) continue;
+        const int i[4] = {e, e | (1 << K1), e | (1 << K0), e | (1 << K0) | (1 << K1)};
+        double2 u[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double2 p = *reinterpret_cast<const double2 *>(c + 2 * i[q]);
+            const double2 v = s[i[q]];
+            u[q] = make_double2(fma(-v.y, p.y, v.x * p.x), fma(v.x, p.y, v.y * p.x));
+        }
+        double2 v0, v1, v2, v3, z[4];
+        rot_pp<0>(u[0], u[1], x1, v0, v1);
+        rot_pp<0>(u[2], u[3], x1, v2, v3);
+        rot_pp<0>(v0, v2, x0, z[0], z[2]);
+        rot_pp<0>(v1, v3, x0, z[1], z[3]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[i[perm[P][q]]] = z[q];
+    }
+}
+
 __device__ __forceinline__ void pp_dtab(const double2 (&s)[16], double2 (&d)[16],
                                         const double *__restrict__ c) {
 #pragma unroll
@@ -286,6 +314,20 @@ __device__ __forceinline__ void pp_apply(const double2 (&s)[16], double2 (&d)[16
         LQ_PR4(0) LQ_PR4(1) LQ_PR4(2) LQ_PR4(3) LQ_PR4(4) LQ_PR4(5)
 #undef LQ_PR4
 #undef LQ_PR
+#define LQ_TP(P, Q)                                                                    \
+    case PC_TPAIR + P * 4 + Q:                                                         \
+        if constexpr (MODE >= 1) {                                                     \
+            const int nv = (op.bits >> 16) & 0xff;                                     \
+            int v = 0;                                                                 \
+            if (nv > 0) v = (int)((gbase >> (op.bits & 0xff)) & 1ull);                 \
+            if (nv > 1) v |= (int)((gbase >> ((op.bits >> 8) & 0xff)) & 1ull) << 1;   \
+            pp_tpair<pair_k0(P), pair_k1(P), Q>(s, d, c + 32 * v, op.x0, op.x1);        \
+        }                                                                              \
+        break;
+#define LQ_TP4(P) LQ_TP(P, 0) LQ_TP(P, 1) LQ_TP(P, 2) LQ_TP(P, 3)
+        LQ_TP4(0) LQ_TP4(1) LQ_TP4(2) LQ_TP4(3) LQ_TP4(4) LQ_TP4(5)
+#undef LQ_TP4
+#undef LQ_TP
     case PC_BLOCK3: if constexpr (MODE >= 2) pp_block<3>(s, d, c); break;
     case PC_BLOCK4: if constexpr (MODE >= 2) pp_block<4>(s, d, c); break;
     default:  // condition false (or an op this MODE does not hold): identity
@@ -342,12 +384,18 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
         const PassOp p0 = ops[o];
         pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
     }
+    if (odd) {  // two store paths: no register moves to bring b into a
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        const uint32_t addr = addr_of(e);
-        const double2 v = odd ? b[e] : a[e];
-        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y)
-                     : "memory");
+        for (int e = 0; e < 16; ++e)
+            asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr_of(e)), "d"(b[e].x),
+                         "d"(b[e].y)
+                         : "memory");
+    } else {
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+            asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr_of(e)), "d"(a[e].x),
+                         "d"(a[e].y)
+                         : "memory");
     }
 }
 
