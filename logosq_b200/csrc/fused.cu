@@ -137,6 +137,7 @@ __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, Ti
                                               const FusedRound *__restrict__ rounds, int nrounds,
                                               const PassOp *__restrict__ ops,
                                               const double *__restrict__ coef,
+                                              const uint16_t *__restrict__ tbtab,
                                               unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -173,7 +174,8 @@ __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, Ti
     }
     const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
     for (int r = 0; r < nrounds; ++r) {
-        run_round_pp<MODE>(tile_a, rounds[r], ops, coef, tile_base, tc.h, tid);
+        const int tbase = tbtab[r * (int)blockDim.x + tid];
+        run_round_pp<MODE>(tile_a, rounds[r], ops, coef, tile_base, tc.h, tbase);
         __syncthreads();
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -194,8 +196,9 @@ template <int MODE>
 __global__ void __launch_bounds__(256, 1)
     k_fused_pp(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                const FusedRound *__restrict__ rounds, int nrounds, const PassOp *__restrict__ ops,
-               const double *__restrict__ coef, unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
+               const double *__restrict__ coef, const uint16_t *__restrict__ tbtab,
+               unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
 }
 
 // 168 registers: six 64-thread CTAs per SM at tile bits 10.  Measured on a
@@ -210,8 +213,8 @@ __global__ void __maxnreg__(LQ_PP_MAXNREG)
     k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                       const FusedRound *__restrict__ rounds, int nrounds,
                       const PassOp *__restrict__ ops, const double *__restrict__ coef,
-                      unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, flag);
+                      const uint16_t *__restrict__ tbtab, unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -1005,7 +1008,8 @@ static int set_pp_attrs() {
 }
 
 static int launch_pass_pp(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
-                          const PassOp *d_ops, const double *d_coef, int mode) {
+                          const PassOp *d_ops, const double *d_coef, const uint16_t *d_tb,
+                          int mode) {
     const int n = s->n;
     const int m = T - 4;
     CUtensorMap map;
@@ -1017,7 +1021,8 @@ static int launch_pass_pp(lq_state *s, int T, int h, const FusedRound *d_rounds,
     prof_begin(s->stream, kProfFused);
     const dim3 blk(1u << (T - 4));
 #define LQ_FUSED_LAUNCH(K) \
-    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, s->d_flag)
+    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, d_tb, \
+                                        s->d_flag)
     (void)mode;  // one op set (4x4, pair and table ops included); blocks use launch_pass
     if (T >= 12) LQ_FUSED_LAUNCH(k_fused_pp<1>);
     else LQ_FUSED_LAUNCH(k_fused_pp_narrow<1>);
@@ -1243,20 +1248,32 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
             fr.op_begin = b0;
             fr.op_end = (int)pops.size();
         }
+        // each thread's tile-local base index, per round (lanes from fill_round)
+        const int nthr = 1 << (T - 4);
+        std::vector<uint16_t> tb(rounds.size() * nthr);
+        for (size_t r = 0; r < rounds.size(); ++r)
+            for (int t = 0; t < nthr; ++t) {
+                int v = 0;
+                for (int j = 0; j < rounds[r].nlane; ++j) v |= ((t >> j) & 1) << rounds[r].lane[j];
+                tb[r * nthr + t] = (uint16_t)v;
+            }
         const size_t rb = rounds.size() * sizeof(FusedRound);
         const size_t ob = pops.size() * sizeof(PassOp);
         const size_t cb = coef.size() * sizeof(double);
+        const size_t tbb = tb.size() * sizeof(uint16_t);
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-        LQ_TRY(ensure_prog(s, al(rb) + al(ob) + al(cb) + 256));
+        LQ_TRY(ensure_prog(s, al(rb) + al(ob) + al(cb) + al(tbb) + 256));
         char *dp = (char *)s->d_prog;
         FusedRound *d_rounds = (FusedRound *)dp;
         PassOp *d_ops = (PassOp *)(dp + al(rb));
         double *d_coef = (double *)(dp + al(rb) + al(ob));
+        uint16_t *d_tb = (uint16_t *)(dp + al(rb) + al(ob) + al(cb));
         // The program buffer may still be read by a previous call's kernels.
         LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
         if (rb) LQ_CUDA_TRY(cudaMemcpy(d_rounds, rounds.data(), rb, cudaMemcpyHostToDevice));
         if (ob) LQ_CUDA_TRY(cudaMemcpy(d_ops, pops.data(), ob, cudaMemcpyHostToDevice));
         if (cb) LQ_CUDA_TRY(cudaMemcpy(d_coef, coef.data(), cb, cudaMemcpyHostToDevice));
+        if (tbb) LQ_CUDA_TRY(cudaMemcpy(d_tb, tb.data(), tbb, cudaMemcpyHostToDevice));
         size_t li = 0;
         for (auto &st : steps) {
             if (!st.fused) {
@@ -1265,8 +1282,8 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
                 continue;
             }
             const PassLaunch &pl = launches[li++];
-            LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops, d_coef,
-                                  pl.mode));
+            LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops,
+                                  d_coef, d_tb + (size_t)pl.round_begin * nthr, pl.mode));
             s->last_launches += 1;
             s->last_passes += 1;
         }

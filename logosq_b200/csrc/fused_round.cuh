@@ -339,13 +339,13 @@ __device__ __forceinline__ void pp_apply(const double2 (&s)[16], double2 (&d)[16
 
 // One round on a tile in shared memory: gather into a, run the ops two at a
 // time (a -> b, b -> a), scatter from the array holding the result.
+// tbase is the thread's tile-local base index in this round (its register
+// bits zero), precomputed on the host from the round's lane order.
 template <int MODE>
 __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &rd,
                                              const PassOp *__restrict__ ops,
                                              const double *__restrict__ coef,
-                                             uint64_t tile_base, int h, int tid) {
-    int tbase = 0;
-    for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
+                                             uint64_t tile_base, int h, int tbase) {
     const uint32_t sb = (uint32_t)swz(tbase) << 4;
     const uint64_t gbase = tile_base | (uint64_t)(tbase & 15) | ((uint64_t)(tbase >> 4) << h);
     // The swizzle is linear over XOR, so element e's offset is the XOR of the
