@@ -1006,7 +1006,8 @@ def main():
     traffic, traffic_q = ncu_traffic("k_fused_pass", n)
     n_u3 = int(np.sum(gates["kind"] == abi.U3))
     fp64_flops_step = 14.0 * n_u3 * (1 << n)  # 2x2 complex matrix: 14 flops per amplitude
-    roofline = {"kernel": "k_fused_pass (TMA-staged 2^T-amplitude tiles)", "bound": "hbm",
+    roofline = {"kernel": "k_fused_pp (TMA-staged 2^T-amplitude tiles, ping-pong register rounds)",
+                "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": 2 * S, "avg_launch_ms": fused_launch_ms,
@@ -1019,7 +1020,9 @@ def main():
                          "frac": fp64_flops_step / (ms_step / 1e3) / 1e12 / FP64_PEAK_TFLOPS,
                          "peak_source": "DFMA throughput probe on this pool's B200",
                          "flops_per_step": fp64_flops_step,
-                         "note": "the fused kernel is FP64 / issue bound"}}
+                         "note": "algorithmic FP64 of the circuit's complex 2x2 gates; the fused "
+                                 "program issues fewer (real folding), and the kernel is latency "
+                                 "bound"}}
 
     # ---- per-gate (unfused) path: one sweep per gate, as Gate::apply --------
     per_gate = None
