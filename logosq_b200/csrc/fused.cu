@@ -132,13 +132,24 @@ __global__ void __maxnreg__(168)
 
 // Ping-pong register rounds (fused_round.cuh) over compact PassOp records;
 // one CTA per tile, as k_fused_pass_narrow.
+// Row length of the per-round thread-base table: the thread count, at least 8
+// entries (16 bytes) so every row starts 16-byte aligned.
+__host__ __device__ __forceinline__ int tb_stride(int nthreads) {
+    return nthreads < 8 ? 8 : nthreads;
+}
+
+// The records [op0, op1) and coefficients [c0, c1) (doubles) one pass reads.
+struct PassRange {
+    int32_t op0, op1, c0, c1;
+};
+
 template <int MODE>
 __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, TileCoords tc,
                                               const FusedRound *__restrict__ rounds, int nrounds,
                                               const PassOp *__restrict__ ops,
                                               const double *__restrict__ coef,
                                               const uint16_t *__restrict__ tbtab,
-                                              unsigned *__restrict__ flag) {
+                                              PassRange pr, unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t tile_bytes = 16u << T;
@@ -164,6 +175,32 @@ __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, Ti
             "l"((uint64_t)&tmap), "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(bar_a)
             : "memory");
     }
+#ifdef LQ_PP_STAGE
+    // While the tile is in flight, copy the pass program (rounds, records,
+    // coefficients, thread bases) into shared memory: every later read of it
+    // is a shared-memory broadcast.
+    {
+        unsigned char *prog = base + tile_bytes + 64;
+        auto stage = [&](unsigned char *dst, const void *src, int bytes) {
+            const int4 *s4 = reinterpret_cast<const int4 *>(src);
+            int4 *d4 = reinterpret_cast<int4 *>(dst);
+            for (int i = tid; i < bytes / 16; i += blockDim.x) d4[i] = s4[i];
+        };
+        const int rb = nrounds * (int)sizeof(FusedRound);
+        const int ob = (pr.op1 - pr.op0) * (int)sizeof(PassOp);
+        const int cb = (pr.c1 - pr.c0) * 8;
+        const int tb = nrounds * tb_stride((int)blockDim.x) * 2;
+        stage(prog, rounds, rb);
+        stage(prog + rb, ops + pr.op0, ob);
+        stage(prog + rb + ob, coef + pr.c0, cb);
+        stage(prog + rb + ob + cb, tbtab, tb);
+        rounds = reinterpret_cast<const FusedRound *>(prog);
+        ops = reinterpret_cast<const PassOp *>(prog + rb) - pr.op0;
+        coef = reinterpret_cast<const double *>(prog + rb + ob) - pr.c0;
+        tbtab = reinterpret_cast<const uint16_t *>(prog + rb + ob + cb);
+        __syncthreads();
+    }
+#endif
     if (!mbar_wait(bar_a, 0)) {
         // leave only once the load no longer targets this CTA's shared memory
         if (tid == 0) {
@@ -174,7 +211,7 @@ __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, Ti
     }
     const uint64_t tile_base = ((uint64_t)c2 << 4) | ((uint64_t)c4 << tc.hm);
     for (int r = 0; r < nrounds; ++r) {
-        const int tbase = tbtab[r * (int)blockDim.x + tid];
+        const int tbase = tbtab[r * tb_stride((int)blockDim.x) + tid];
         run_round_pp<MODE>(tile_a, rounds[r], ops, coef, tile_base, tc.h, tbase);
         __syncthreads();
     }
@@ -197,8 +234,8 @@ __global__ void __launch_bounds__(256, 1)
     k_fused_pp(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                const FusedRound *__restrict__ rounds, int nrounds, const PassOp *__restrict__ ops,
                const double *__restrict__ coef, const uint16_t *__restrict__ tbtab,
-               unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
+               PassRange pr, unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, pr, flag);
 }
 
 // 168 registers: six 64-thread CTAs per SM at tile bits 10.  Measured on a
@@ -213,8 +250,9 @@ __global__ void __maxnreg__(LQ_PP_MAXNREG)
     k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                       const FusedRound *__restrict__ rounds, int nrounds,
                       const PassOp *__restrict__ ops, const double *__restrict__ coef,
-                      const uint16_t *__restrict__ tbtab, unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
+                      const uint16_t *__restrict__ tbtab, PassRange pr,
+                      unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, pr, flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -998,7 +1036,7 @@ static PassOp pass_op(const FusedOp &f) {
 static int set_pp_attrs() {
     static bool done = false;
     if (done) return LQ_OK;
-    const int mx = (int)fused_smem(kMaxT);
+    const int mx = 227 * 1024;
 #define LQ_ATTR(K) LQ_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
     LQ_ATTR(k_fused_pp<1>);
     LQ_ATTR(k_fused_pp_narrow<1>);
@@ -1009,19 +1047,24 @@ static int set_pp_attrs() {
 
 static int launch_pass_pp(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
                           const PassOp *d_ops, const double *d_coef, const uint16_t *d_tb,
-                          int mode) {
+                          PassRange pr, int mode) {
     const int n = s->n;
     const int m = T - 4;
     CUtensorMap map;
     LQ_TRY(make_tile_map(&map, s->d, n, h, m));
     const int ntiles = 1 << (n - T);
     TileCoords tc{h, h + m, ntiles};
-    const size_t smem = fused_smem(T);
+    size_t smem = fused_smem(T);
+#ifdef LQ_PP_STAGE
+    smem += 64 + nrounds * sizeof(FusedRound) + (size_t)(pr.op1 - pr.op0) * sizeof(PassOp) +
+            (size_t)(pr.c1 - pr.c0) * 8 + (size_t)nrounds * tb_stride(1 << (T - 4)) * 2;
+    if (smem > 227 * 1024) return set_error(LQ_ERR_UNSUPPORTED, "fused pass program too large");
+#endif
     LQ_TRY(set_pp_attrs());
     prof_begin(s->stream, kProfFused);
     const dim3 blk(1u << (T - 4));
 #define LQ_FUSED_LAUNCH(K) \
-    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, d_tb, \
+    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, d_tb, pr, \
                                         s->d_flag)
     (void)mode;  // one op set (4x4, pair and table ops included); blocks use launch_pass
     if (T >= 12) LQ_FUSED_LAUNCH(k_fused_pp<1>);
@@ -1249,13 +1292,13 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
             fr.op_end = (int)pops.size();
         }
         // each thread's tile-local base index, per round (lanes from fill_round)
-        const int nthr = 1 << (T - 4);
-        std::vector<uint16_t> tb(rounds.size() * nthr);
+        const int nthr = 1 << (T - 4), stride = tb_stride(nthr);
+        std::vector<uint16_t> tb(rounds.size() * stride, 0);
         for (size_t r = 0; r < rounds.size(); ++r)
             for (int t = 0; t < nthr; ++t) {
                 int v = 0;
                 for (int j = 0; j < rounds[r].nlane; ++j) v |= ((t >> j) & 1) << rounds[r].lane[j];
-                tb[r * nthr + t] = (uint16_t)v;
+                tb[r * stride + t] = (uint16_t)v;
             }
         const size_t rb = rounds.size() * sizeof(FusedRound);
         const size_t ob = pops.size() * sizeof(PassOp);
@@ -1282,8 +1325,26 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
                 continue;
             }
             const PassLaunch &pl = launches[li++];
+            PassRange pr{0, 0, 0, 0};
+            if (pl.nrounds > 0) {
+                pr.op0 = rounds[pl.round_begin].op_begin;
+                pr.op1 = rounds[pl.round_begin + pl.nrounds - 1].op_end;
+                int c0 = (int)coef.size(), c1 = 0;
+                for (int o = pr.op0; o < pr.op1; ++o) {
+                    const int span = (pops[o].code == PC_DTAB ||
+                                      (pops[o].code >= PC_TPAIR && pops[o].code < PC_COUNT))
+                                         ? 32 << ((pops[o].bits >> 16) & 0xff)
+                                         : 32;
+                    c0 = std::min(c0, pops[o].coef);
+                    c1 = std::max(c1, std::min(pops[o].coef + span, (int)coef.size()));
+                }
+                c0 &= ~1;  // 16-byte aligned copy
+                pr.c0 = std::min(c0, c1);
+                pr.c1 = (c1 + 1) & ~1;
+                if (pr.c1 > (int)((coef.size() + 1) & ~1ull)) pr.c1 = (int)coef.size() & ~1;
+            }
             LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops,
-                                  d_coef, d_tb + (size_t)pl.round_begin * nthr, pl.mode));
+                                  d_coef, d_tb + (size_t)pl.round_begin * stride, pr, pl.mode));
             s->last_launches += 1;
             s->last_passes += 1;
         }
