@@ -138,18 +138,13 @@ __host__ __device__ __forceinline__ int tb_stride(int nthreads) {
     return nthreads < 8 ? 8 : nthreads;
 }
 
-// The records [op0, op1) and coefficients [c0, c1) (doubles) one pass reads.
-struct PassRange {
-    int32_t op0, op1, c0, c1;
-};
-
 template <int MODE>
 __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, TileCoords tc,
                                               const FusedRound *__restrict__ rounds, int nrounds,
                                               const PassOp *__restrict__ ops,
                                               const double *__restrict__ coef,
                                               const uint16_t *__restrict__ tbtab,
-                                              PassRange pr, unsigned *__restrict__ flag) {
+                                              unsigned *__restrict__ flag) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t tile_bytes = 16u << T;
@@ -175,32 +170,6 @@ __device__ __forceinline__ void fused_pp_body(const CUtensorMap &tmap, int T, Ti
             "l"((uint64_t)&tmap), "r"(zero), "r"(zero), "r"(c2), "r"(zero), "r"(c4), "r"(bar_a)
             : "memory");
     }
-#ifdef LQ_PP_STAGE
-    // While the tile is in flight, copy the pass program (rounds, records,
-    // coefficients, thread bases) into shared memory: every later read of it
-    // is a shared-memory broadcast.
-    {
-        unsigned char *prog = base + tile_bytes + 64;
-        auto stage = [&](unsigned char *dst, const void *src, int bytes) {
-            const int4 *s4 = reinterpret_cast<const int4 *>(src);
-            int4 *d4 = reinterpret_cast<int4 *>(dst);
-            for (int i = tid; i < bytes / 16; i += blockDim.x) d4[i] = s4[i];
-        };
-        const int rb = nrounds * (int)sizeof(FusedRound);
-        const int ob = (pr.op1 - pr.op0) * (int)sizeof(PassOp);
-        const int cb = (pr.c1 - pr.c0) * 8;
-        const int tb = nrounds * tb_stride((int)blockDim.x) * 2;
-        stage(prog, rounds, rb);
-        stage(prog + rb, ops + pr.op0, ob);
-        stage(prog + rb + ob, coef + pr.c0, cb);
-        stage(prog + rb + ob + cb, tbtab, tb);
-        rounds = reinterpret_cast<const FusedRound *>(prog);
-        ops = reinterpret_cast<const PassOp *>(prog + rb) - pr.op0;
-        coef = reinterpret_cast<const double *>(prog + rb + ob) - pr.c0;
-        tbtab = reinterpret_cast<const uint16_t *>(prog + rb + ob + cb);
-        __syncthreads();
-    }
-#endif
     if (!mbar_wait(bar_a, 0)) {
         // leave only once the load no longer targets this CTA's shared memory
         if (tid == 0) {
@@ -234,8 +203,8 @@ __global__ void __launch_bounds__(256, 1)
     k_fused_pp(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                const FusedRound *__restrict__ rounds, int nrounds, const PassOp *__restrict__ ops,
                const double *__restrict__ coef, const uint16_t *__restrict__ tbtab,
-               PassRange pr, unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, pr, flag);
+               unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
 }
 
 // 168 registers: six 64-thread CTAs per SM at tile bits 10.  Measured on a
@@ -250,9 +219,8 @@ __global__ void __maxnreg__(LQ_PP_MAXNREG)
     k_fused_pp_narrow(const __grid_constant__ CUtensorMap tmap, int T, TileCoords tc,
                       const FusedRound *__restrict__ rounds, int nrounds,
                       const PassOp *__restrict__ ops, const double *__restrict__ coef,
-                      const uint16_t *__restrict__ tbtab, PassRange pr,
-                      unsigned *__restrict__ flag) {
-    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, pr, flag);
+                      const uint16_t *__restrict__ tbtab, unsigned *__restrict__ flag) {
+    fused_pp_body<MODE>(tmap, T, tc, rounds, nrounds, ops, coef, tbtab, flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -1036,7 +1004,7 @@ static PassOp pass_op(const FusedOp &f) {
 static int set_pp_attrs() {
     static bool done = false;
     if (done) return LQ_OK;
-    const int mx = 227 * 1024;
+    const int mx = (int)fused_smem(kMaxT);
 #define LQ_ATTR(K) LQ_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
     LQ_ATTR(k_fused_pp<1>);
     LQ_ATTR(k_fused_pp_narrow<1>);
@@ -1047,24 +1015,19 @@ static int set_pp_attrs() {
 
 static int launch_pass_pp(lq_state *s, int T, int h, const FusedRound *d_rounds, int nrounds,
                           const PassOp *d_ops, const double *d_coef, const uint16_t *d_tb,
-                          PassRange pr, int mode) {
+                          int mode) {
     const int n = s->n;
     const int m = T - 4;
     CUtensorMap map;
     LQ_TRY(make_tile_map(&map, s->d, n, h, m));
     const int ntiles = 1 << (n - T);
     TileCoords tc{h, h + m, ntiles};
-    size_t smem = fused_smem(T);
-#ifdef LQ_PP_STAGE
-    smem += 64 + nrounds * sizeof(FusedRound) + (size_t)(pr.op1 - pr.op0) * sizeof(PassOp) +
-            (size_t)(pr.c1 - pr.c0) * 8 + (size_t)nrounds * tb_stride(1 << (T - 4)) * 2;
-    if (smem > 227 * 1024) return set_error(LQ_ERR_UNSUPPORTED, "fused pass program too large");
-#endif
+    const size_t smem = fused_smem(T);
     LQ_TRY(set_pp_attrs());
     prof_begin(s->stream, kProfFused);
     const dim3 blk(1u << (T - 4));
 #define LQ_FUSED_LAUNCH(K) \
-    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, d_tb, pr, \
+    K<<<ntiles, blk, smem, s->stream>>>(map, T, tc, d_rounds, nrounds, d_ops, d_coef, d_tb, \
                                         s->d_flag)
     (void)mode;  // one op set (4x4, pair and table ops included); blocks use launch_pass
     if (T >= 12) LQ_FUSED_LAUNCH(k_fused_pp<1>);
@@ -1325,26 +1288,8 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
                 continue;
             }
             const PassLaunch &pl = launches[li++];
-            PassRange pr{0, 0, 0, 0};
-            if (pl.nrounds > 0) {
-                pr.op0 = rounds[pl.round_begin].op_begin;
-                pr.op1 = rounds[pl.round_begin + pl.nrounds - 1].op_end;
-                int c0 = (int)coef.size(), c1 = 0;
-                for (int o = pr.op0; o < pr.op1; ++o) {
-                    const int span = (pops[o].code == PC_DTAB ||
-                                      (pops[o].code >= PC_TPAIR && pops[o].code < PC_COUNT))
-                                         ? 32 << ((pops[o].bits >> 16) & 0xff)
-                                         : 32;
-                    c0 = std::min(c0, pops[o].coef);
-                    c1 = std::max(c1, std::min(pops[o].coef + span, (int)coef.size()));
-                }
-                c0 &= ~1;  // 16-byte aligned copy
-                pr.c0 = std::min(c0, c1);
-                pr.c1 = (c1 + 1) & ~1;
-                if (pr.c1 > (int)((coef.size() + 1) & ~1ull)) pr.c1 = (int)coef.size() & ~1;
-            }
             LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops,
-                                  d_coef, d_tb + (size_t)pl.round_begin * stride, pr, pl.mode));
+                                  d_coef, d_tb + (size_t)pl.round_begin * stride, pl.mode));
             s->last_launches += 1;
             s->last_passes += 1;
         }
