@@ -199,9 +199,25 @@ __global__ void __launch_bounds__(kTcThreads, 2)
             : "memory");
     };
 
+    // B hi + lo of block bi: one 32 KiB bulk copy of the host-prepared swizzled image
+    auto issue_b = [&](int bi) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b),
+                     "r"(2 * kBBytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+            " [%0], [%1], %2, [%3];" ::"r"(tc_smem_u32(b_hi)),
+            "l"((uint64_t)(bimg + blocks[bi].b_offset)), "r"(2 * kBBytes), "r"(bar_b)
+            : "memory");
+    };
+
     uint32_t load_phase[2] = {0u, 0u}, b_phase = 0u, mma_phase = 0u;
     bool load_pending[2] = {false, false};  // thread 0: a tile load not yet waited for
-    bool mma_pending = false;
+    bool mma_pending = false, b_pending = false;
+    if (tid == 0 && (int)blockIdx.x < ntiles && nblocks > 0) {
+        issue_b(0);
+        b_pending = true;
+    }
     int buf = 0;
     if (tid == 0 && (int)blockIdx.x < ntiles) {
         issue_load(blockIdx.x, 0);
@@ -224,16 +240,8 @@ __global__ void __launch_bounds__(kTcThreads, 2)
         const uint32_t tile_a = tc_smem_u32(tile);
         for (int bi = 0; bi < nblocks; ++bi) {
             const TcBlock &blk = blocks[bi];
-            if (tid == 0) {  // B hi + lo: one 32 KiB bulk copy (prepared swizzled image)
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b),
-                             "r"(2 * kBBytes)
-                             : "memory");
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-                    " [%0], [%1], %2, [%3];" ::"r"(tc_smem_u32(b_hi)),
-                    "l"((uint64_t)(bimg + blk.b_offset)), "r"(2 * kBBytes), "r"(bar_b)
-                    : "memory");
-            }
+            // (this block's B image was requested when the previous block's MMAs
+            // had finished reading the buffer, or before the first tile)
             // A row m = tid: the block's 32 complex entries, split hi / lo into TMEM
             uint32_t lbase = 0;
 #pragma unroll
@@ -262,6 +270,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 if (!tc_wait(bar_b, b_phase)) {
                     atomicExch(s_abort, 1);
                 } else {
+                    b_pending = false;
                     const uint32_t bh = tc_smem_u32(b_hi), bl = tc_smem_u32(b_lo);
 #pragma unroll
                     for (int prod = 0; prod < 3; ++prod) {
@@ -298,7 +307,16 @@ __global__ void __launch_bounds__(kTcThreads, 2)
             __syncthreads();
             if (*s_abort) break;
             mma_phase ^= 1u;
-            if (tid == 0) mma_pending = false;
+            if (tid == 0) {
+                mma_pending = false;
+                // the MMAs have read B: request the next block's image now, so the
+                // copy overlaps this block's readback and the next block's split
+                const int nb = bi + 1 < nblocks ? bi + 1 : 0;
+                if (bi + 1 < nblocks || t + (int)gridDim.x < ntiles) {
+                    issue_b(nb);
+                    b_pending = true;
+                }
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             // D row m = tid back into the tile
 #pragma unroll
@@ -335,6 +353,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
             atomicOr(flag, kFlagTimeout);
             // let work in flight finish before the CTA's memory is released
             if (mma_pending) tc_wait(bar_mma, mma_phase);
+            if (b_pending) tc_wait(bar_b, b_phase);
             for (int b = 0; b < 2; ++b)
                 if (load_pending[b]) tc_wait(bar_load0 + 8u * b, load_phase[b]);
         }
