@@ -246,13 +246,22 @@ __global__ void __launch_bounds__(kTcThreads, 2)
             uint32_t lbase = 0;
 #pragma unroll
             for (int j = 0; j < 7; ++j) lbase |= (((uint32_t)tid >> j) & 1u) << blk.row_bits[j];
+            // tile_off is linear over XOR on disjoint bits: the offset of column c is
+            // the XOR of the offsets of its five block bits (five loads, not 32)
+            const uint32_t rowoff = tile_off(lbase);
+            const uint32_t cb0 = tile_off(1u << blk.k[0]), cb1 = tile_off(1u << blk.k[1]),
+                           cb2 = tile_off(1u << blk.k[2]), cb3 = tile_off(1u << blk.k[3]),
+                           cb4 = tile_off(1u << blk.k[4]);
+            auto col_off = [&](int c) {
+                return ((c & 1) ? cb0 : 0u) ^ ((c & 2) ? cb1 : 0u) ^ ((c & 4) ? cb2 : 0u) ^
+                       ((c & 8) ? cb3 : 0u) ^ ((c & 16) ? cb4 : 0u);
+            };
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float hi[16], lo[16];
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
-                    const uint32_t l = lbase | blocks[bi].col_bits[q * 8 + c];
-                    const float2 v = *(const float2 *)(tile + tile_off(l));
+                    const float2 v = *(const float2 *)(tile + (rowoff ^ col_off(q * 8 + c)));
                     const float rh = to_tf32(v.x), ih = to_tf32(v.y);
                     hi[2 * c] = rh;
                     hi[2 * c + 1] = ih;
@@ -326,8 +335,8 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
-                    const uint32_t l = lbase | blocks[bi].col_bits[q * 8 + c];
-                    *(float2 *)(tile + tile_off(l)) = make_float2(d[2 * c], d[2 * c + 1]);
+                    *(float2 *)(tile + (rowoff ^ col_off(q * 8 + c))) =
+                        make_float2(d[2 * c], d[2 * c + 1]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
