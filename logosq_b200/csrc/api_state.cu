@@ -43,6 +43,7 @@ int check_qubit(const lq_state *s, int q) {
 }
 
 int ensure_prog(lq_state *s, size_t bytes) {
+    s->prog_valid = false;  // the caller is about to write the buffer
     if (s->prog_cap >= bytes) return LQ_OK;
     if (s->d_prog) {
         LQ_CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -948,6 +949,7 @@ int lq_state_destroy(lq_state *s) {
     if (s->h_red) cudaFreeHost(s->h_red);
     if (s->d_flag) cudaFree(s->d_flag);
     if (s->d_prog) cudaFree(s->d_prog);
+    free_plan_cache(s);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return LQ_OK;

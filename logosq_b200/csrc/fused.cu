@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <atomic>
 #include <complex>
+#include <memory>
 #include <mutex>
 
 #include "fused_plan.h"
@@ -1200,17 +1201,78 @@ static void encode_steps(const std::vector<PlanStep> &steps, const std::vector<G
     }
 }
 
+// ---------------------------------------------------------------------------
+// Plan cache: the program of the last fused circuit stays in the handle's
+// program buffer with its launch list, so submitting the same circuit again
+// (same gates, angles and settings, compared byte for byte) launches at once:
+// no planning, no upload, no synchronisation with earlier work.
+// ---------------------------------------------------------------------------
+struct PlanCache {
+    std::vector<unsigned char> key;
+    int T = 0, stride = 0;
+    size_t off_ops = 0, off_coef = 0, off_tb = 0;
+    struct Step {
+        bool fused;
+        GateOp gate;
+        PassLaunch pl;
+    };
+    std::vector<Step> steps;
+};
+
+void free_plan_cache(lq_state *s) {
+    delete static_cast<PlanCache *>(s->plan_cache);
+    s->plan_cache = nullptr;
+    s->prog_valid = false;
+}
+
+static std::vector<unsigned char> plan_key(const lq_gate *ops, int nops, const double *theta,
+                                           int ntheta, int n, int T) {
+    const int32_t hdr[6] = {n, T, nops, ntheta, real_fold_mode(), pp_engine()};
+    std::vector<unsigned char> k(sizeof(hdr) + sizeof(lq_gate) * (size_t)nops +
+                                 sizeof(double) * (size_t)ntheta);
+    memcpy(k.data(), hdr, sizeof(hdr));
+    if (nops) memcpy(k.data() + sizeof(hdr), ops, sizeof(lq_gate) * (size_t)nops);
+    if (ntheta)
+        memcpy(k.data() + sizeof(hdr) + sizeof(lq_gate) * (size_t)nops, theta,
+               sizeof(double) * (size_t)ntheta);
+    return k;
+}
+
+static int launch_cached(lq_state *s, const PlanCache &pc) {
+    const char *dp = (const char *)s->d_prog;
+    const FusedRound *d_rounds = (const FusedRound *)dp;
+    const PassOp *d_ops = (const PassOp *)(dp + pc.off_ops);
+    const double *d_coef = (const double *)(dp + pc.off_coef);
+    const uint16_t *d_tb = (const uint16_t *)(dp + pc.off_tb);
+    for (const auto &st : pc.steps) {
+        if (!st.fused) {
+            LQ_TRY(launch_gate_op(s, st.gate));
+            s->last_launches += st.gate.renorm ? 3 : 1;
+            continue;
+        }
+        LQ_TRY(launch_pass_pp(s, pc.T, st.pl.h, d_rounds + st.pl.round_begin, st.pl.nrounds, d_ops,
+                              d_coef, d_tb + (size_t)st.pl.round_begin * pc.stride, st.pl.mode));
+        s->last_launches += 1;
+        s->last_passes += 1;
+    }
+    return LQ_OK;
+}
+
 int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *theta,
                        int ntheta, int mode) {
     const int n = s->n;
     s->last_launches = 0;
     s->last_passes = 0;
-    std::vector<GateOp> gops(nops);
-    for (int i = 0; i < nops; ++i) {
-        LQ_TRY(validate_gate(&ops[i], n, ntheta));
-        LQ_TRY(make_gate_op(&ops[i], theta, n, &gops[i]));
-    }
+    for (int i = 0; i < nops; ++i) LQ_TRY(validate_gate(&ops[i], n, ntheta));
     const bool can_fuse = mode == LQ_EXEC_FUSED && s->dtype == LQ_C128 && n >= 5;
+    std::vector<unsigned char> key;
+    if (can_fuse && pp_engine() == 1) {
+        key = plan_key(ops, nops, theta, ntheta, n, std::min(fusion_width(), n));
+        const PlanCache *pc = static_cast<const PlanCache *>(s->plan_cache);
+        if (s->prog_valid && pc && pc->key == key) return launch_cached(s, *pc);
+    }
+    std::vector<GateOp> gops(nops);
+    for (int i = 0; i < nops; ++i) LQ_TRY(make_gate_op(&ops[i], theta, n, &gops[i]));
     if (!can_fuse) {
         for (int i = 0; i < nops; ++i) {
             LQ_TRY(launch_gate_op(s, gops[i]));
@@ -1280,20 +1342,22 @@ int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *
         if (ob) LQ_CUDA_TRY(cudaMemcpy(d_ops, pops.data(), ob, cudaMemcpyHostToDevice));
         if (cb) LQ_CUDA_TRY(cudaMemcpy(d_coef, coef.data(), cb, cudaMemcpyHostToDevice));
         if (tbb) LQ_CUDA_TRY(cudaMemcpy(d_tb, tb.data(), tbb, cudaMemcpyHostToDevice));
+        auto pc = std::make_unique<PlanCache>();
+        pc->key = std::move(key);
+        pc->T = T;
+        pc->stride = stride;
+        pc->off_ops = (size_t)((char *)d_ops - dp);
+        pc->off_coef = (size_t)((char *)d_coef - dp);
+        pc->off_tb = (size_t)((char *)d_tb - dp);
         size_t li = 0;
         for (auto &st : steps) {
-            if (!st.fused) {
-                LQ_TRY(launch_gate_op(s, gops[st.gate]));
-                s->last_launches += gops[st.gate].renorm ? 3 : 1;
-                continue;
-            }
-            const PassLaunch &pl = launches[li++];
-            LQ_TRY(launch_pass_pp(s, T, pl.h, d_rounds + pl.round_begin, pl.nrounds, d_ops,
-                                  d_coef, d_tb + (size_t)pl.round_begin * stride, pl.mode));
-            s->last_launches += 1;
-            s->last_passes += 1;
+            if (!st.fused) pc->steps.push_back({false, gops[st.gate], PassLaunch{}});
+            else pc->steps.push_back({true, GateOp{}, launches[li++]});
         }
-        return LQ_OK;
+        free_plan_cache(s);
+        s->plan_cache = pc.release();
+        s->prog_valid = true;
+        return launch_cached(s, *static_cast<const PlanCache *>(s->plan_cache));
     }
     const size_t rb = rounds.size() * sizeof(FusedRound);
     const size_t ob = fops.size() * sizeof(FusedOp);

@@ -73,6 +73,11 @@ struct lq_state {
     // Statistics of the last circuit call.
     int last_launches = 0;
     int last_passes = 0;
+    // The fused program now in d_prog and its launch list, kept so that the same
+    // circuit submitted again skips planning and the upload (fused.cu).  Any
+    // other writer of d_prog goes through ensure_prog, which clears prog_valid.
+    void *plan_cache = nullptr;
+    bool prog_valid = false;
 };
 
 namespace lq {
@@ -115,6 +120,7 @@ void prof_begin(cudaStream_t st, int cls);
 void prof_end(cudaStream_t st, int cls);
 
 // fused.cu
+void free_plan_cache(lq_state *s);
 int apply_circuit_impl(lq_state *s, const lq_gate *ops, int nops, const double *theta,
                        int ntheta, int mode);
 int apply_block_impl(lq_state *s, int k, const int *qubits, const double *m);
