@@ -378,6 +378,11 @@ int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits);
  * 2^12 amplitudes, or 0 to autotune again on the next lq_batch_gradients call.
  * No reference counterpart (tuning control of this engine). */
 int lq_batch_set_tile_bits(lq_batch *b, int tile_bits);
+/* Whether the batch shares circuit prefixes (each shifted circuit starts from
+ * the unshifted circuit's state just before its parameter's first gate; off
+ * when LQ_BATCH_PREFIX=0 at creation or when the checkpoints would not fit)
+ * and the device bytes its checkpoints take.  No reference counterpart. */
+int lq_batch_prefix_info(const lq_batch *b, int *shared, uint64_t *checkpoint_bytes);
 
 /* ---------------------------------------------------------------------------
  * Noise models (NoiseModel::apply, src/noise/mod.rs) on complex128 states.

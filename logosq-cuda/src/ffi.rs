@@ -154,6 +154,7 @@ extern "C" {
     pub fn lq_batch_gradients(b: *mut LqBatch, theta: *const f64, shift: f64, energy: *mut f64, grad: *mut f64) -> c_int;
     pub fn lq_batch_tuning(b: *const LqBatch, smem_max_qubits: *mut c_int, tile_bits: *mut c_int) -> c_int;
     pub fn lq_batch_set_tile_bits(b: *mut LqBatch, tile_bits: c_int) -> c_int;
+    pub fn lq_batch_prefix_info(b: *const LqBatch, shared: *mut c_int, checkpoint_bytes: *mut u64) -> c_int;
     pub fn lq_noise_pauli(s: *mut LqState, qubit: c_int, pauli: c_int) -> c_int;
     pub fn lq_noise_amplitude_damping(s: *mut LqState, gamma: f64, qubits: *const c_int, nqubits: c_int) -> c_int;
     pub fn lq_noise_phase_damping(s: *mut LqState, lambda: f64, qubits: *const c_int, nqubits: c_int) -> c_int;

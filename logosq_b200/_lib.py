@@ -92,6 +92,7 @@ _PROTOS = {
     "lq_batch_num_params": (C.c_int, [_P, _PI]),
     "lq_batch_gradients": (C.c_int, [_P, _PD, C.c_double, _PD, _PD]),
     "lq_batch_tuning": (C.c_int, [_P, _PI, _PI]),
+    "lq_batch_prefix_info": (C.c_int, [_P, _PI, C.POINTER(C.c_uint64)]),
     "lq_batch_set_tile_bits": (C.c_int, [_P, C.c_int]),
     "lq_noise_pauli": (C.c_int, [_P, C.c_int, C.c_int]),
     "lq_noise_amplitude_damping": (C.c_int, [_P, C.c_double, _PI, C.c_int]),

@@ -69,7 +69,10 @@ class BatchedParameterShift:
     def tuning(self):
         a, b = C.c_int(), C.c_int()
         call("lq_batch_tuning", self._h, C.byref(a), C.byref(b))
-        return {"smem_max_qubits": a.value, "tile_bits": b.value}
+        c, d = C.c_int(), C.c_uint64()
+        call("lq_batch_prefix_info", self._h, C.byref(c), C.byref(d))
+        return {"smem_max_qubits": a.value, "tile_bits": b.value,
+                "shared_prefixes": bool(c.value), "checkpoint_bytes": d.value}
 
 
 def heisenberg_batch(instances, layers=4):

@@ -29,6 +29,7 @@ struct BInst {
     int32_t pass_begin, npass;
     int32_t ewin_begin, newin;
     int32_t coef_base;  // offset of the instance's coefficient block
+    int64_t ckpt_off;   // first amplitude of the instance's checkpoints
 };
 
 struct BPass {
@@ -59,7 +60,9 @@ struct BItem {
     int32_t inst;
     int32_t param;  // -1: unshifted
     int32_t sign;   // +1 / -1
-    int32_t pad;
+    int32_t spass;  // first pass to run
+    int32_t sround; // first round of that pass
+    int32_t src;    // checkpoint holding the state before it (-1: |0...0>)
 };
 
 struct BProgram {  // device program for one fusion width
@@ -78,6 +81,18 @@ struct BProgram {  // device program for one fusion width
     std::vector<std::vector<PlanStep>> steps;
     std::vector<int> op_begin;  // first fop of each instance
     std::vector<int> nops;
+    std::vector<BPass> h_passes;
+    // per instance and parameter: the (pass, round) holding the first op bound
+    // to it (pass = npass when no op is)
+    std::vector<std::vector<std::pair<int, int>>> first_use;
+    // work items (the base circuits first when prefixes are shared) and the
+    // checkpoint index of the state after each round (-1: none kept)
+    BItem *items = nullptr;
+    std::vector<BItem> h_items;
+    int nbase = 0;
+    int32_t *rckpt = nullptr;
+    std::vector<int32_t> h_rckpt;
+    size_t ckpt_amps = 0;
 };
 
 }  // namespace lq
@@ -93,8 +108,10 @@ struct lq_batch {
     lq::BEWin *ewins = nullptr;
     lq::BGroup *groups = nullptr;
     lq::BTerm *bterms = nullptr;
-    lq::BItem *items = nullptr;
     int nitems = 0;
+    bool share_prefix = false;  // shifted circuits start from the base circuit's checkpoints
+    double2 *ckpt = nullptr;
+    size_t ckpt_amps = 0;
     double *coef_d = nullptr;
     double *coef_h = nullptr;  // pinned
     size_t coef_cap = 0;
@@ -178,11 +195,12 @@ __device__ double tile_energy(uint32_t tile_a, int T, int h, uint64_t tile_base,
     return acc;
 }
 
-__device__ __forceinline__ void gather_tile(uint32_t tile_a, const double2 *__restrict__ slot,
+// src == nullptr reads the state |0...0> without touching memory.
+__device__ __forceinline__ void gather_tile(uint32_t tile_a, const double2 *__restrict__ src,
                                             int T, int h, uint64_t tile_base, int tid) {
     for (int l = tid; l < (1 << T); l += kBatchThreads) {
         const uint64_t g = tile_base | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h);
-        const double2 v = slot[g];
+        const double2 v = src ? src[g] : make_double2(g == 0 ? 1.0 : 0.0, 0.0);
         asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(tile_a + ((uint32_t)swz(l) << 4)),
                      "d"(v.x), "d"(v.y)
                      : "memory");
@@ -207,7 +225,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             const FusedOp *__restrict__ ops, const double *__restrict__ coef,
             const BEWin *__restrict__ ewins, const BGroup *__restrict__ groups,
             const BTerm *__restrict__ terms, double *__restrict__ energy,
-            unsigned *__restrict__ counter, double2 *__restrict__ scratch, size_t slot_amps) {
+            unsigned *__restrict__ counter, double2 *__restrict__ scratch, size_t slot_amps,
+            const int32_t *__restrict__ rckpt, double2 *__restrict__ ckpt) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t tile_a = smem_u32(base);
@@ -236,25 +255,23 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         const int T = in.T;
         const int nthr = 1 << (T - 4);
         double acc = 0.0;
+        // A shifted circuit shares every gate before its parameter's first op with
+        // the base (unshifted) circuit: it starts at that op's (pass, round) from
+        // the base circuit's checkpoint of the state just before it.  The base
+        // circuit writes those checkpoints (2^n amplitudes each, natural order).
+        const bool base_item = cur_p < 0;
+        const size_t N = (size_t)1 << in.n;
+        double2 *ck = ckpt + in.ckpt_off;
+        const double2 *src = item.src >= 0 ? ck + (size_t)item.src * N : nullptr;
         // n <= 12: the whole state is one tile in shared memory; otherwise it
         // lives in this CTA's HBM slot and every pass sweeps it tile by tile.
         // One code path for both keeps a single inlined copy of the register
         // rounds (register pressure).  Only the 2^(T-4) threads that own
         // amplitudes run a round.
         const bool in_smem = in.n <= kSmemStateMax;
-        if (in_smem) {
-            for (int l = tid; l < (1 << T); l += kBatchThreads) {
-                const double re = l == 0 ? 1.0 : 0.0;
-                asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(tile_a +
-                                                                       ((uint32_t)swz(l) << 4)),
-                             "d"(re), "d"(0.0)
-                             : "memory");
-            }
-        } else {
-            const uint64_t N = 1ull << in.n;
-            for (uint64_t i = tid; i < N; i += kBatchThreads)
-                slot[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
-        }
+        // (in shared memory T = n and h = 4, so tile element l is amplitude l; a
+        // state in the HBM slot is read from src by the first pass's gathers)
+        if (in_smem) gather_tile(tile_a, src, T, 4, 0ull, tid);
         __syncthreads();
         const int ntiles = in_smem ? 1 : 1 << (in.n - T);
         auto tile_base = [&](int t, int h) -> uint64_t {
@@ -263,15 +280,19 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             const uint64_t c4 = (uint64_t)(t >> (h - 4));
             return (c2 << 4) | (c4 << (h + T - 4));
         };
-        for (int p = 0; p < in.npass; ++p) {
+        for (int p = item.spass; p < in.npass; ++p) {
             const BPass ps = passes[in.pass_begin + p];
+            const int r0 = p == item.spass ? item.sround : 0;
+            // the base circuit's pass-end checkpoint takes the place of the slot
+            const int cend = base_item ? rckpt[ps.round_begin + ps.nrounds - 1] : -1;
+            double2 *dst = cend >= 0 ? ck + (size_t)cend * N : slot;
             for (int t = 0; t < ntiles; ++t) {
                 const uint64_t tb = tile_base(t, ps.h);
                 if (!in_smem) {
-                    gather_tile(tile_a, slot, T, ps.h, tb, tid);
+                    gather_tile(tile_a, src, T, ps.h, tb, tid);
                     __syncthreads();
                 }
-                for (int r = 0; r < ps.nrounds; ++r) {
+                for (int r = r0; r < ps.nrounds; ++r) {
                     // A branch around the round costs the full-width case (all 256
                     // threads own amplitudes) much of its speed: give it its own
                     // unconditional copy.
@@ -282,19 +303,27 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                         run_round<0>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb,
                                      ps.h, tid);
                     __syncthreads();
+                    if (base_item) {
+                        const int ci = rckpt[ps.round_begin + r];
+                        if (ci >= 0 && (in_smem || r + 1 < ps.nrounds)) {
+                            scatter_tile(tile_a, ck + (size_t)ci * N, T, ps.h, tb, tid);
+                            __syncthreads();
+                        }
+                    }
                 }
                 if (!in_smem) {
-                    scatter_tile(tile_a, slot, T, ps.h, tb, tid);
+                    scatter_tile(tile_a, dst, T, ps.h, tb, tid);
                     __syncthreads();
                 }
             }
+            if (!in_smem) src = dst;
         }
         for (int w = 0; w < in.newin; ++w) {
             const BEWin ew = ewins[in.ewin_begin + w];
             for (int t = 0; t < ntiles; ++t) {
                 const uint64_t tb = tile_base(t, ew.h);
                 if (!in_smem) {
-                    gather_tile(tile_a, slot, T, ew.h, tb, tid);
+                    gather_tile(tile_a, src, T, ew.h, tb, tid);
                     __syncthreads();
                 }
                 acc += tile_energy(tile_a, T, ew.h, tb, groups, ew.group_begin, ew.ngroups, terms,
@@ -547,6 +576,18 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
                 alt += 16;
             }
         }
+        // first (pass, round) of each parameter's ops, in execution order
+        std::vector<std::pair<int, int>> fu(b->nparams[i], {in.npass, 0});
+        for (int k = 0; k < in.npass; ++k) {
+            const BPass &bp = passes[in.pass_begin + k];
+            for (int r = 0; r < bp.nrounds; ++r) {
+                const FusedRound &fr = rounds[bp.round_begin + r];
+                for (int o = fr.op_begin; o < fr.op_end; ++o)
+                    for (int q : {fops[o].param, fops[o].param2})
+                        if (q >= 0 && fu[q].first == in.npass) fu[q] = {k, r};
+            }
+        }
+        pg.first_use.push_back(std::move(fu));
         in.coef_base = (int)coef_off;
         coef_off += alt;
         pg.steps[i] = std::move(steps);
@@ -554,6 +595,8 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     }
     pg.ncoef = coef_off;
     pg.h_ops = fops;
+    pg.h_passes = passes;
+    pg.h_rckpt.assign(rounds.size(), -1);
     // energy windows are shared by the programs (set in lq_batch_create)
     LQ_CUDA_TRY(cudaMalloc(&pg.rounds, sizeof(FusedRound) * std::max<size_t>(rounds.size(), 1)));
     LQ_CUDA_TRY(cudaMalloc(&pg.ops, sizeof(FusedOp) * std::max<size_t>(fops.size(), 1)));
@@ -566,6 +609,74 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     LQ_CUDA_TRY(cudaMemcpy(pg.passes, passes.data(), sizeof(BPass) * passes.size(),
                            cudaMemcpyHostToDevice));
     return LQ_OK;
+}
+
+// Work items and checkpoints of program pg.  Without shared prefixes every
+// circuit runs from |0...0> in one launch.  With them the base circuits run
+// first, in a launch of their own, keeping per instance the state just before
+// each parameter's first op (after round r-1 of its pass, or after the previous
+// pass); each shifted circuit then starts at that op from that checkpoint, so
+// the gates before it are applied once per instance instead of once per
+// circuit.  The sums are the same in the same order, so the energies are
+// bitwise those of the unshared launch.
+static void plan_items(lq_batch *b, BProgram &pg, bool share) {
+    std::fill(pg.h_rckpt.begin(), pg.h_rckpt.end(), -1);
+    pg.h_items.clear();
+    std::vector<BItem> shifted;
+    size_t amps = 0;
+    for (int i = 0; i < b->ninst; ++i) {
+        BInst &in = pg.h_insts[i];
+        in.ckpt_off = (int64_t)amps;
+        pg.h_items.push_back(BItem{i, -1, 1, 0, 0, -1});
+        auto round_index = [&](int k, int r) {
+            return pg.h_passes[in.pass_begin + k].round_begin + r;
+        };
+        int nck = 0;
+        for (int p = 0; p < in.nparams; ++p) {
+            int k = 0, r = 0, src = -1;
+            const std::pair<int, int> fu = pg.first_use[i][p];
+            if (share && fu.first < in.npass) {
+                k = fu.first;
+                r = fu.second;
+                int gr = -1;
+                if (r > 0)
+                    gr = round_index(k, r - 1);
+                else if (k > 0)
+                    gr = round_index(k - 1, pg.h_passes[in.pass_begin + k - 1].nrounds - 1);
+                if (gr >= 0) {
+                    if (pg.h_rckpt[gr] < 0) pg.h_rckpt[gr] = nck++;
+                    src = pg.h_rckpt[gr];
+                }
+            }
+            for (int sg : {1, -1}) shifted.push_back(BItem{i, p, sg, k, r, src});
+        }
+        amps += (size_t)nck << in.n;
+    }
+    // largest remaining work first (passes carry a tile sweep each, rounds the
+    // register work, the energy windows a sweep each)
+    auto cost = [&](const BItem &it) {
+        const BInst &in = pg.h_insts[it.inst];
+        double w = 2.0 * in.newin - it.sround;
+        for (int k = it.spass; k < in.npass; ++k)
+            w += 4.0 + pg.h_passes[in.pass_begin + k].nrounds;
+        return std::ldexp(w, in.n);
+    };
+    if (share) {
+        std::stable_sort(pg.h_items.begin(), pg.h_items.end(), [&](const BItem &x, const BItem &y) {
+            return b->n[x.inst] > b->n[y.inst];
+        });
+        std::stable_sort(shifted.begin(), shifted.end(),
+                         [&](const BItem &x, const BItem &y) { return cost(x) > cost(y); });
+        pg.nbase = (int)pg.h_items.size();
+        pg.h_items.insert(pg.h_items.end(), shifted.begin(), shifted.end());
+    } else {
+        pg.h_items.insert(pg.h_items.end(), shifted.begin(), shifted.end());
+        std::stable_sort(pg.h_items.begin(), pg.h_items.end(), [&](const BItem &x, const BItem &y) {
+            return b->n[x.inst] > b->n[y.inst];
+        });
+        pg.nbase = 0;
+    }
+    pg.ckpt_amps = share ? amps : 0;
 }
 
 // Host FP64 coefficients of every instance for parameter vector theta.
@@ -609,15 +720,23 @@ static int fill_coefficients(lq_batch *b, BProgram &pg, const double *theta, dou
 }
 
 static int launch_batch(lq_batch *b, BProgram &pg) {
-    LQ_CUDA_TRY(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
+    LQ_CUDA_TRY(cudaMemsetAsync(b->counter, 0, 2 * sizeof(unsigned), b->stream));
     LQ_CUDA_TRY(cudaMemcpyAsync(b->coef_d, b->coef_h, pg.ncoef * sizeof(double),
                                 cudaMemcpyHostToDevice, b->stream));
     prof_begin(b->stream, kProfBatch);
-    k_batch<<<b->grid, kBatchThreads, batch_smem(), b->stream>>>(
-        b->items, b->nitems, pg.insts, pg.passes, pg.rounds, pg.ops, b->coef_d, b->ewins,
-        b->groups, b->bterms, b->energy_d, b->counter, b->scratch, b->slot_amps);
+    // items [0, nbase): the base circuits, which write the checkpoints that the
+    // shifted circuits [nbase, nitems) start from (stream order between the two)
+    const int bounds[3] = {0, pg.nbase, b->nitems};
+    for (int ph = 0; ph < 2; ++ph) {
+        const int i0 = bounds[ph], cnt = bounds[ph + 1] - bounds[ph];
+        if (cnt <= 0) continue;
+        k_batch<<<b->grid, kBatchThreads, batch_smem(), b->stream>>>(
+            pg.items + i0, cnt, pg.insts, pg.passes, pg.rounds, pg.ops, b->coef_d, b->ewins,
+            b->groups, b->bterms, b->energy_d + i0, b->counter + ph, b->scratch, b->slot_amps,
+            pg.rckpt, b->ckpt);
+        LQ_CUDA_TRY(cudaGetLastError());
+    }
     prof_end(b->stream, kProfBatch);
-    LQ_CUDA_TRY(cudaGetLastError());
     LQ_CUDA_TRY(cudaMemcpyAsync(b->energy_h, b->energy_d, b->nitems * sizeof(double),
                                 cudaMemcpyDeviceToHost, b->stream));
     return LQ_OK;
@@ -631,11 +750,13 @@ static void free_batch(lq_batch *b) {
         cudaFree(pg.ops);
         cudaFree(pg.passes);
         cudaFree(pg.insts);
+        cudaFree(pg.items);
+        cudaFree(pg.rckpt);
     }
+    cudaFree(b->ckpt);
     cudaFree(b->ewins);
     cudaFree(b->groups);
     cudaFree(b->bterms);
-    cudaFree(b->items);
     cudaFree(b->coef_d);
     if (b->coef_h) cudaFreeHost(b->coef_h);
     cudaFree(b->energy_d);
@@ -695,6 +816,29 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
         int rc = build_program(b, Tw, pg);
         b->progs.push_back(pg);
         if (rc) return fail(rc);
+    }
+    // Shared prefixes (LQ_BATCH_PREFIX=0 turns them off) need the checkpoints
+    // of the largest program to fit next to the scratch slots.
+    {
+        const char *ev = getenv("LQ_BATCH_PREFIX");
+        b->share_prefix = !(ev && atoi(ev) == 0);
+        size_t need = 0;
+        for (auto &pg : b->progs) {
+            plan_items(b, pg, b->share_prefix);
+            need = std::max(need, pg.ckpt_amps);
+        }
+        size_t freeb = 0, totalb = 0;
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const size_t slots = b->maxn > kSmemStateMax ? (size_t)2 * nsm << b->maxn : 0;
+        if (b->share_prefix && (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess ||
+                                (need + slots) * sizeof(double2) > freeb / 10 * 8)) {
+            b->share_prefix = false;
+            for (auto &pg : b->progs) plan_items(b, pg, false);
+            need = 0;
+        }
+        b->ckpt_amps = need;
     }
     // Energy windows and term groups (shared by all programs: they only depend on
     // the instance's tile width, which is <= 12 ... windows use T of program 0 for
@@ -758,18 +902,7 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
                        cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return fail(set_error(LQ_ERR_CUDA, "%s", cudaGetErrorString(e)));
     }
-    // Work items, largest qubit count first.
-    std::vector<BItem> items;
-    for (int i = 0; i < b->ninst; ++i) {
-        items.push_back(BItem{i, -1, 1, 0});
-        for (int p = 0; p < b->nparams[i]; ++p) {
-            items.push_back(BItem{i, p, 1, 0});
-            items.push_back(BItem{i, p, -1, 0});
-        }
-    }
-    std::stable_sort(items.begin(), items.end(),
-                     [&](const BItem &x, const BItem &y) { return b->n[x.inst] > b->n[y.inst]; });
-    b->nitems = (int)items.size();
+    b->nitems = (int)b->progs[0].h_items.size();
     size_t maxcoef = 0;
     for (auto &pg : b->progs) maxcoef = std::max(maxcoef, pg.ncoef);
     b->coef_cap = std::max<size_t>(maxcoef, 1);
@@ -788,12 +921,21 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
     LQ_B_TRY(cudaMalloc(&b->ewins, sizeof(BEWin) * std::max<size_t>(ewins.size(), 1)));
     LQ_B_TRY(cudaMalloc(&b->groups, sizeof(BGroup) * std::max<size_t>(groups.size(), 1)));
     LQ_B_TRY(cudaMalloc(&b->bterms, sizeof(BTerm) * std::max<size_t>(bterms.size(), 1)));
-    LQ_B_TRY(cudaMalloc(&b->items, sizeof(BItem) * items.size()));
+    for (auto &pg : b->progs) {
+        LQ_B_TRY(cudaMalloc(&pg.items, sizeof(BItem) * pg.h_items.size()));
+        LQ_B_TRY(cudaMalloc(&pg.rckpt, sizeof(int32_t) * std::max<size_t>(pg.h_rckpt.size(), 1)));
+        LQ_B_TRY(cudaMemcpy(pg.items, pg.h_items.data(), sizeof(BItem) * pg.h_items.size(),
+                            cudaMemcpyHostToDevice));
+        if (!pg.h_rckpt.empty())
+            LQ_B_TRY(cudaMemcpy(pg.rckpt, pg.h_rckpt.data(), sizeof(int32_t) * pg.h_rckpt.size(),
+                                cudaMemcpyHostToDevice));
+    }
+    LQ_B_TRY(cudaMalloc(&b->ckpt, sizeof(double2) * std::max<size_t>(b->ckpt_amps, 1)));
     LQ_B_TRY(cudaMalloc(&b->coef_d, sizeof(double) * b->coef_cap));
     LQ_B_TRY(cudaMallocHost(&b->coef_h, sizeof(double) * b->coef_cap));
     LQ_B_TRY(cudaMalloc(&b->energy_d, sizeof(double) * b->nitems));
     LQ_B_TRY(cudaMallocHost(&b->energy_h, sizeof(double) * b->nitems));
-    LQ_B_TRY(cudaMalloc(&b->counter, sizeof(unsigned)));
+    LQ_B_TRY(cudaMalloc(&b->counter, 2 * sizeof(unsigned)));
     LQ_B_TRY(cudaMalloc(&b->flag, sizeof(unsigned)));
     LQ_B_TRY(cudaMalloc(&b->scratch, sizeof(double2) * b->slot_amps * b->grid));
     if (!ewins.empty())
@@ -805,8 +947,6 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
     if (!bterms.empty())
         LQ_B_TRY(cudaMemcpy(b->bterms, bterms.data(), sizeof(BTerm) * bterms.size(),
                             cudaMemcpyHostToDevice));
-    LQ_B_TRY(cudaMemcpy(b->items, items.data(), sizeof(BItem) * items.size(),
-                        cudaMemcpyHostToDevice));
     LQ_B_TRY(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)batch_smem()));
 #undef LQ_B_TRY
@@ -872,9 +1012,7 @@ int lq_batch_gradients(lq_batch *b, const double *theta, double shift, double *e
     LQ_CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
     LQ_CUDA_TRY(cudaStreamSynchronize(b->stream));
     // gradients (E(+s) - E(-s)) / 2 from the item energies
-    std::vector<BItem> items(b->nitems);
-    LQ_CUDA_TRY(cudaMemcpy(items.data(), b->items, sizeof(BItem) * b->nitems,
-                           cudaMemcpyDeviceToHost));
+    const std::vector<BItem> &items = pg.h_items;
     std::vector<double> ep(b->total_params), em(b->total_params);
     for (int k = 0; k < b->nitems; ++k) {
         const BItem &it = items[k];
@@ -896,6 +1034,13 @@ int lq_batch_tuning(const lq_batch *b, int *smem_max_qubits, int *tile_bits) {
     if (!b) return set_error(LQ_ERR_INVALID_ARG, "null batch");
     if (smem_max_qubits) *smem_max_qubits = kSmemStateMax;
     if (tile_bits) *tile_bits = b->chosen >= 0 ? b->progs[b->chosen].T : 0;
+    return LQ_OK;
+}
+
+int lq_batch_prefix_info(const lq_batch *b, int *shared, uint64_t *checkpoint_bytes) {
+    if (!b) return set_error(LQ_ERR_INVALID_ARG, "null batch");
+    if (shared) *shared = b->share_prefix ? 1 : 0;
+    if (checkpoint_bytes) *checkpoint_bytes = (uint64_t)b->ckpt_amps * sizeof(double2);
     return LQ_OK;
 }
 

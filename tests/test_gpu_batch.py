@@ -105,3 +105,81 @@ def test_batch_set_tile_bits_rejects_unknown_width():
         call("lq_batch_set_tile_bits", b._h, 9)
     assert e.value.code == abi.LQ_ERR_INVALID_ARG
     call("lq_batch_set_tile_bits", b._h, 0)  # back to autotuning
+
+
+def _make(recs, share, templates=None, extra_params=0):
+    import os
+    from logosq_b200.batch import BatchedParameterShift
+    old = os.environ.get("LQ_BATCH_PREFIX")
+    os.environ["LQ_BATCH_PREFIX"] = "1" if share else "0"
+    try:
+        specs = []
+        for k, r in enumerate(recs):
+            n = r["n"]
+            g = templates[k] if templates else workloads.basic_entangling_template(n, 4)
+            specs.append((n, g, 8 * n + extra_params,
+                          workloads.heisenberg_terms(n, r["jx"], r["jy"], r["jz"], r["h"])))
+        return BatchedParameterShift(specs)
+    finally:
+        if old is None:
+            del os.environ["LQ_BATCH_PREFIX"]
+        else:
+            os.environ["LQ_BATCH_PREFIX"] = old
+
+
+@pytest.mark.parametrize("tile_bits", [10, 11, 12])
+def test_shared_prefixes_are_bitwise_the_unshared_launch(tile_bits):
+    """Shifted circuits that start from the base circuit's checkpoints give
+    exactly the energies of circuits run from |0...0> (same sums, same order),
+    for states in shared memory (n <= 12) and in HBM slots (n > 12)."""
+    recs = workloads.heisenberg_instances(10, seed=31, n_lo=9, n_hi=15)
+    theta = np.concatenate([r["theta"] for r in recs])
+    out = {}
+    for share in (True, False):
+        b = _make(recs, share)
+        call("lq_batch_set_tile_bits", b._h, tile_bits)
+        info = b.tuning()
+        assert info["shared_prefixes"] == share
+        assert (info["checkpoint_bytes"] > 0) == share
+        out[share] = b.gradients(theta)
+        e2, g2 = b.gradients(theta + 0.05)  # the graph replays with new angles
+        out[(share, 1)] = (e2, g2)
+    assert np.array_equal(out[True][0], out[False][0])
+    assert np.array_equal(out[True][1], out[False][1])
+    assert np.array_equal(out[(True, 1)][1], out[(False, 1)][1])
+    # and the plain path agrees
+    gs = np.split(out[True][1], np.cumsum([8 * r["n"] for r in recs])[:-1])
+    for i in (0, len(recs) - 1):
+        r = recs[i]
+        n = r["n"]
+        _, g_plain = plain_gradient(n, workloads.basic_entangling_template(n, 4), r["theta"],
+                                    workloads.heisenberg_terms(n, r["jx"], r["jy"], r["jz"],
+                                                               r["h"]))
+        assert np.abs(gs[i] - g_plain).max() < 1e-10
+
+
+def test_shared_prefixes_with_reused_and_unused_parameters():
+    """A parameter bound to gates in two layers starts at its first gate; a
+    parameter bound to none keeps a zero gradient."""
+    recs = workloads.heisenberg_instances(3, seed=41, n_lo=11, n_hi=14)
+    temps = []
+    for r in recs:
+        g = workloads.basic_entangling_template(r["n"], 4).copy()
+        ry = np.nonzero(g["kind"] == abi.RY)[0]
+        g["param"][ry[-1], 0] = g["param"][ry[0], 0]  # last RY reuses parameter 0
+        temps.append(g)
+    P = [8 * r["n"] + 1 for r in recs]
+    rng = np.random.default_rng(3)
+    theta = rng.uniform(-np.pi, np.pi, sum(P))
+    res = {s: _make(recs, s, temps, extra_params=1).gradients(theta) for s in (True, False)}
+    assert np.array_equal(res[True][1], res[False][1])
+    gs = np.split(res[True][1], np.cumsum(P)[:-1])
+    off = 0
+    for i, r in enumerate(recs):
+        n = r["n"]
+        th = theta[off:off + P[i]]
+        off += P[i]
+        g_or = oracle.parameter_shift(n, temps[i], th, workloads.heisenberg_terms(
+            n, r["jx"], r["jy"], r["jz"], r["h"]))
+        assert np.abs(gs[i] - g_or).max() < 1e-10
+        assert gs[i][-1] == 0.0

@@ -49,7 +49,7 @@ def test_repeat_and_invalidation():
         # a block gate rewrites the buffer too
         u, _ = np.linalg.qr(np.random.default_rng(1).normal(size=(8, 8)) + 0j)
         m = np.ascontiguousarray(u).view(np.float64).reshape(-1)
-        qs = (C.c_int * 3)(0, 5, 9)
+        qs = (C.c_int * 3)(13, 8, 6)  # index bits 0, 5, 7
         call("lq_apply_block", st.handle, 3, qs, m.ctypes.data_as(C.POINTER(C.c_double)))
         got_block = st.vector()
         run(st, n, g1)

@@ -2,7 +2,7 @@
 
 One 5-qubit block is a complex 32x32 matrix applied to 128 rows of a tile, i.e.
 the real product X' W' (X' 128 x 64, W' 64 x 64).  TF32 keeps 10 explicit
-mantissa bits (cvt.rna: round to nearest, ties away).  Emulated here in
+mantissa bits (round to nearest, ties away, as the kernel rounds).  Emulated here in
 numpy with exact products and FP64 sums (the tensor cores' products are exact;
 their sums are FP32): plain TF32 operands leave a relative error near 2^-11,
 far above the 1e-5 block bar of tests/test_gpu_tc.py, while the 3xTF32 split
