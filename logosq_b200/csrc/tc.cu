@@ -76,10 +76,15 @@ __device__ __forceinline__ uint32_t tile_off(uint32_t l) {
     return row * 128 + ((chunk ^ (row & 7)) << 4) + ((l & 1) << 3);
 }
 
+// Round a finite FP32 value to TF32 (10 explicit mantissa bits), to nearest with
+// ties away from zero: add half a unit of the last kept place (bit 12) to the
+// IEEE bit pattern and clear the 13 dropped bits.  The pattern is
+// sign-magnitude, so the same addition rounds negative values by magnitude, and
+// a carry out of the mantissa steps into the next binade as rounding up should.
+// Two integer operations instead of a conversion sequence that also handles
+// NaN and infinity, which amplitudes (magnitude at most 1) never are.
 __device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 __device__ __forceinline__ uint64_t make_sdesc(uint32_t addr, uint32_t sbo_bytes) {
@@ -256,17 +261,31 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 return ((c & 1) ? cb0 : 0u) ^ ((c & 2) ? cb1 : 0u) ^ ((c & 4) ? cb2 : 0u) ^
                        ((c & 8) ? cb3 : 0u) ^ ((c & 16) ? cb4 : 0u);
             };
+            // Block bit 0 on tile bit 0: columns 2c, 2c+1 share a 16-byte chunk
+            // (one 128-bit access for both, and the lane bits then cover the
+            // chunk slots without bank conflicts).
+            const bool pair = blk.k[0] == 0;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 float hi[16], lo[16];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const float2 v = *(const float2 *)(tile + (rowoff ^ col_off(q * 8 + c)));
-                    const float rh = to_tf32(v.x), ih = to_tf32(v.y);
-                    hi[2 * c] = rh;
-                    hi[2 * c + 1] = ih;
-                    lo[2 * c] = to_tf32(v.x - rh);
-                    lo[2 * c + 1] = to_tf32(v.y - ih);
+                for (int c = 0; c < 8; c += 2) {
+                    float4 v;
+                    if (pair) {
+                        v = *(const float4 *)(tile + (rowoff ^ col_off(q * 8 + c)));
+                    } else {
+                        const float2 v0 = *(const float2 *)(tile + (rowoff ^ col_off(q * 8 + c)));
+                        const float2 v1 =
+                            *(const float2 *)(tile + (rowoff ^ col_off(q * 8 + c + 1)));
+                        v = make_float4(v0.x, v0.y, v1.x, v1.y);
+                    }
+                    const float x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const float hx = to_tf32(x[u]);
+                        hi[2 * c + u] = hx;
+                        lo[2 * c + u] = to_tf32(x[u] - hx);
+                    }
                 }
                 tmem_st16(lane_base + kColAh + q * 16, hi);
                 tmem_st16(lane_base + kColAl + q * 16, lo);
@@ -334,9 +353,16 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 tmem_ld16(lane_base + kColD + q * 16, d);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    *(float2 *)(tile + (rowoff ^ col_off(q * 8 + c))) =
-                        make_float2(d[2 * c], d[2 * c + 1]);
+                for (int c = 0; c < 8; c += 2) {
+                    unsigned char *p0 = tile + (rowoff ^ col_off(q * 8 + c));
+                    if (pair) {
+                        *(float4 *)p0 = make_float4(d[2 * c], d[2 * c + 1], d[2 * c + 2],
+                                                    d[2 * c + 3]);
+                    } else {
+                        *(float2 *)p0 = make_float2(d[2 * c], d[2 * c + 1]);
+                        *(float2 *)(tile + (rowoff ^ col_off(q * 8 + c + 1))) =
+                            make_float2(d[2 * c + 2], d[2 * c + 3]);
+                    }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -613,6 +639,11 @@ int apply_circuit_tc_impl(lq_state *s, const lq_gate *ops, int nops, const doubl
         for (size_t b = 0; b < bl.size(); ++b) {
             int gbit[5];
             for (int j = 0; j < 5; ++j) gbit[j] = bb[b][j];
+            // A block on tile bit 0 takes it as its block bit 0: columns 2c and
+            // 2c+1 are then the two halves of one 16-byte chunk, read and written
+            // as a pair.  U is built in this bit order, so the order is free.
+            for (int j = 1; j < 5; ++j)
+                if (local_pos(gbit[j], st.pass.h) == 0) std::swap(gbit[0], gbit[j]);
             // block unitary U (32 x 32): column e = product of gates on basis e
             cd U[32][32];
             for (int e = 0; e < 32; ++e) {
