@@ -795,6 +795,41 @@ def run_learned(args):
             t_plain[n] = time.perf_counter() - tt
         st.close()
 
+    # The plain arm measured end to end on a sample: the first chains, from
+    # their random starts, through the per-circuit API (one energy and one
+    # parameter-shift gradient per iteration, Adam on the host) until the
+    # energy is within 1e-3 of E* or eval_iters updates have run.
+    sample = []
+    for i in range(min(args.plain_sample, len(ev))):
+        r = ev[i]
+        n = r["n"]
+        gates = workloads.basic_entangling_template(n, 4)
+        terms = learned.chain_terms(r)
+        th = np.array(starts["random"][i], dtype=np.float64)
+        mo, vo = np.zeros_like(th), np.zeros_like(th)
+        gp = np.zeros(len(th))
+        e = C.c_double()
+        st = State.zero_state(n)
+        tt = time.perf_counter()
+        steps_run = iters
+        for it in range(1, iters + 2):
+            common = (st.handle, abi.gate_ptr(gates), len(gates), abi.f64_ptr(th), len(th),
+                      abi.term_ptr(terms), len(terms), abi.Y_REFERENCE)
+            call("lq_ansatz_energy", *common, C.byref(e))
+            if e.value - best[i] < 1e-3 or it == iters + 1:
+                steps_run = it - 1
+                break
+            call("lq_parameter_shift", *common, math.pi / 2, abi.f64_ptr(gp))
+            mo = 0.9 * mo + 0.1 * gp
+            vo = 0.999 * vo + 0.001 * gp * gp
+            th -= 0.05 * (mo / (1 - 0.9 ** it)) / (np.sqrt(vo / (1 - 0.999 ** it)) + 1e-8)
+        wall = time.perf_counter() - tt
+        st.close()
+        modelled = min(int(its["random"][1e-3][i]), cap) * t_plain[n]
+        sample.append({"n": n, "updates": steps_run,
+                       "batched_trace_updates": int(its["random"][1e-3][i]),
+                       "measured_s": wall, "modelled_s": modelled})
+
     # Wall time to the target, each chain charged only its own iterations (capped
     # at eval_iters + 1 when it never gets there): on the batched engine one
     # chain-iteration costs the chunk's measured seconds per iteration divided
@@ -862,6 +897,11 @@ def run_learned(args):
             "batched_random_wall_s_to_target": batched_random,
             "warm_batched_wall_s_to_target": warm_batched,
             "plain_s_per_iteration_by_qubits": t_plain,
+            "plain_measured_sample": {
+                "chains": sample,
+                "measured_over_modelled": (sum(c["measured_s"] for c in sample) /
+                                           max(sum(c["modelled_s"] for c in sample), 1e-30))
+                if sample else None},
             "starts": summary,
             "to_random_init_final_energy": match,
             "exact": {"min_gap_best_to_E0": float((best - E0).min()),
@@ -928,6 +968,8 @@ def main():
     ap.add_argument("--eval-iters", type=int, default=300)
     ap.add_argument("--eval-starts", default="random,fixed_small_angle,supervised_only,warm",
                     help="learned form: the starts evaluated (random and warm always)")
+    ap.add_argument("--plain-sample", type=int, default=8,
+                    help="learned form: chains whose plain per-circuit VQE is run end to end")
     ap.add_argument("--family", default="disordered", choices=["disordered", "independent"],
                     help="learned form: coupling family of the chains")
     ap.add_argument("--save-traces", default=None,
