@@ -54,6 +54,8 @@ struct BGroup {
 struct BTerm {
     uint64_t z;
     double ca, cb;
+    int32_t p;    // X-mask-0 group: Z bits on tile bits 8..T-1 (terms sorted by it)
+    uint32_t lz;  // Z bits inside the window, in tile-local positions
 };
 
 struct BItem {
@@ -141,56 +143,133 @@ __device__ __forceinline__ uint64_t insert_zero_u(uint64_t x, int pos) {
     return ((x >> pos) << (pos + 1)) | lo;
 }
 
-// Energy contribution of the groups of one window over the tile in smem.
+__device__ __forceinline__ uint32_t insert_zero32(uint32_t x, int pos) {
+    return ((x >> pos) << (pos + 1)) | (x & ((1u << pos) - 1));
+}
+
+__device__ __forceinline__ double2 tile_amp(uint32_t tile_a, int l) {
+    double2 a;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(a.x), "=d"(a.y)
+                 : "r"(tile_a + ((uint32_t)swz(l) << 4)));
+    return a;
+}
+
+// c[k] <- sum_p c[p] (-1)^popcount(k & p), the 16-point Walsh-Hadamard transform.
+__device__ __forceinline__ void wht16(double (&c)[16]) {
+#pragma unroll
+    for (int s = 1; s < 16; s <<= 1)
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (!(k & s)) {
+                const double x = c[k], y = c[k | s];
+                c[k] = x + y;
+                c[k | s] = x - y;
+            }
+}
+
+// Energy contribution of the groups of one window over the tile in smem
+// (kBatchThreads threads).  A term's Z sign at global index g is the sign of
+// the bits outside the window (tile_base) times the sign of the tile-local bits
+// (its lz), so per-term work that depends only on the tile is done once per tile.
 __device__ double tile_energy(uint32_t tile_a, int T, int h, uint64_t tile_base,
                               const BGroup *__restrict__ groups, int g0, int ng,
-                              const BTerm *__restrict__ terms, int tid, int nthr) {
+                              const BTerm *__restrict__ terms, int tid) {
+    constexpr int nthr = kBatchThreads;
     double acc = 0.0;
-    const int m = T - 4;
     for (int g = g0; g < g0 + ng; ++g) {
         const BGroup gr = groups[g];
         const uint32_t lx = gr.lx;
         const BTerm *tp = terms + gr.term_begin;
-        if (lx == 0) {
+        const int nt = gr.nterms;
+        if (lx == 0 && T >= 8) {
+            // Diagonal group, folded.  This thread's amplitudes l = tid + 256 k
+            // (k < 2^(T-8)) differ only in tile bits 8..T-1; a term's sign is the
+            // sign of the fixed bits (gfix) times (-1)^popcount(k & p), p = its Z
+            // bits there.  Terms arrive sorted by p, so each thread sums them
+            // into c[p] and one Walsh-Hadamard transform gives the coefficient of
+            // every k: a few operations per amplitude instead of a popcount and a
+            // select per term per amplitude.
+            const uint64_t gfix =
+                tile_base | (uint64_t)(tid & 15) | ((uint64_t)(tid >> 4) << h);
+            double c[16];
+            int t = 0;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                double sum = 0.0;
+                for (; t < nt && tp[t].p == q; ++t)
+                    sum += (__popcll(gfix & tp[t].z) & 1) ? -tp[t].ca : tp[t].ca;
+                c[q] = sum;
+            }
+            wht16(c);
+            const int nv = 1 << (T - 8);
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (k < nv) {
+                    const double2 a = tile_amp(tile_a, tid + (k << 8));
+                    acc += (a.x * a.x + a.y * a.y) * c[k];
+                }
+        } else if (lx == 0) {
             for (int l = tid; l < (1 << T); l += nthr) {
-                const uint64_t gi = tile_base | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h);
-                double2 a;
-                asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
-                             : "=d"(a.x), "=d"(a.y)
-                             : "r"(tile_a + ((uint32_t)swz(l) << 4)));
+                const double2 a = tile_amp(tile_a, l);
                 double alpha = 0.0;
-                for (int t = 0; t < gr.nterms; ++t)
-                    alpha += ((__popcll(gi & tp[t].z) & 1) ? -tp[t].ca : tp[t].ca);
+                for (int t = 0; t < nt; ++t) {
+                    const bool sg = (__popcll(tile_base & tp[t].z) + __popc((uint32_t)l & tp[t].lz)) & 1;
+                    alpha += sg ? -tp[t].ca : tp[t].ca;
+                }
                 acc += (a.x * a.x + a.y * a.y) * alpha;
             }
         } else {
+            // Pairs (l, l ^ lx), l with bit hb clear.  The j-side sums follow from
+            // the i side: a term's Z sign at j is its sign at i times (-1)^ny, and
+            // ca = 0 for odd ny, cb = 0 for even ny, so aj = ai and bj = -bi.
             const int hb = 31 - __clz(lx);
-            for (int p = tid; p < (1 << (T - 1)); p += nthr) {
-                const int l = (int)insert_zero_u((uint64_t)p, hb);
-                const int j = l ^ (int)lx;
-                const uint64_t gi = tile_base | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h);
-                double2 a, b;
-                asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
-                             : "=d"(a.x), "=d"(a.y)
-                             : "r"(tile_a + ((uint32_t)swz(l) << 4)));
-                asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
-                             : "=d"(b.x), "=d"(b.y)
-                             : "r"(tile_a + ((uint32_t)swz(j) << 4)));
-                const double wr = a.x * b.x + a.y * b.y;
-                const double wi = a.x * b.y - a.y * b.x;
-                // The j-side sums follow from the i side: a term's Z sign at j is
-                // its sign at i times (-1)^ny, and ca = 0 for odd ny, cb = 0 for
-                // even ny, so aj = ai and bj = -bi.
-                double ai = 0.0, bi = 0.0;
-                for (int t = 0; t < gr.nterms; ++t) {
-                    const bool si = __popcll(gi & tp[t].z) & 1;
-                    ai += si ? -tp[t].ca : tp[t].ca;
-                    bi += si ? -tp[t].cb : tp[t].cb;
+            if (nt <= 2) {
+                // up to two terms (XX and YY of a bond): coefficients with the
+                // sign of their fixed bits, once per tile, in registers
+                uint32_t lz0 = 0, lz1 = 0;
+                double ca0 = 0.0, cb0 = 0.0, ca1 = 0.0, cb1 = 0.0;
+                {
+                    const BTerm t0 = tp[0];
+                    const bool f = __popcll(tile_base & t0.z) & 1;
+                    lz0 = t0.lz;
+                    ca0 = f ? -t0.ca : t0.ca;
+                    cb0 = f ? -t0.cb : t0.cb;
                 }
-                acc += 2.0 * (wr * ai + wi * bi);
+                if (nt > 1) {
+                    const BTerm t1 = tp[1];
+                    const bool f = __popcll(tile_base & t1.z) & 1;
+                    lz1 = t1.lz;
+                    ca1 = f ? -t1.ca : t1.ca;
+                    cb1 = f ? -t1.cb : t1.cb;
+                }
+                for (int p = tid; p < (1 << (T - 1)); p += nthr) {
+                    const uint32_t l = insert_zero32((uint32_t)p, hb);
+                    const double2 a = tile_amp(tile_a, (int)l), b = tile_amp(tile_a, (int)(l ^ lx));
+                    const double wr = a.x * b.x + a.y * b.y;
+                    const double wi = a.x * b.y - a.y * b.x;
+                    const bool s0 = __popc(l & lz0) & 1, s1 = __popc(l & lz1) & 1;
+                    const double ai = (s0 ? -ca0 : ca0) + (s1 ? -ca1 : ca1);
+                    const double bi = (s0 ? -cb0 : cb0) + (s1 ? -cb1 : cb1);
+                    acc += 2.0 * (wr * ai + wi * bi);
+                }
+            } else {
+                for (int p = tid; p < (1 << (T - 1)); p += nthr) {
+                    const uint32_t l = insert_zero32((uint32_t)p, hb);
+                    const double2 a = tile_amp(tile_a, (int)l), b = tile_amp(tile_a, (int)(l ^ lx));
+                    const double wr = a.x * b.x + a.y * b.y;
+                    const double wi = a.x * b.y - a.y * b.x;
+                    double ai = 0.0, bi = 0.0;
+                    for (int t = 0; t < nt; ++t) {
+                        const bool si =
+                            (__popcll(tile_base & tp[t].z) + __popc(l & tp[t].lz)) & 1;
+                        ai += si ? -tp[t].ca : tp[t].ca;
+                        bi += si ? -tp[t].cb : tp[t].cb;
+                    }
+                    acc += 2.0 * (wr * ai + wi * bi);
+                }
             }
         }
-        (void)m;
     }
     return acc;
 }
@@ -327,7 +406,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                     __syncthreads();
                 }
                 acc += tile_energy(tile_a, T, ew.h, tb, groups, ew.group_begin, ew.ngroups, terms,
-                                   tid, kBatchThreads);
+                                   tid);
                 if (!in_smem) __syncthreads();  // before the next gather overwrites the tile
             }
         }
@@ -885,13 +964,26 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
                     for (int bt = 0; bt < n; ++bt)
                         if ((x >> bt) & 1) lx |= 1u << (bt < 4 ? bt : 4 + (bt - w.first));
                     BGroup g{x, (int)bterms.size(), (int)byx[x].size(), lx, 0};
+                    const int h = w.first;
+                    const uint64_t wm = window_mask(h, m);
+                    std::vector<BTerm> gt;
                     for (int t : byx[x]) {
                         const lq_pauli_term &pt = b->terms[i][t];
                         int k = pt.ny & 3;  // reference convention: Y = +i
                         const double a = k == 0 ? 1.0 : k == 2 ? -1.0 : 0.0;
                         const double bb = k == 1 ? -1.0 : k == 3 ? 1.0 : 0.0;
-                        bterms.push_back(BTerm{pt.zmask, pt.coefficient * a, pt.coefficient * bb});
+                        uint32_t lz = 0;  // Z bits inside the window, tile-local
+                        for (int bt = 0; bt < n; ++bt)
+                            if ((pt.zmask & wm) >> bt & 1) lz |= 1u << (bt < 4 ? bt : 4 + (bt - h));
+                        // the diagonal group's fold index: Z bits on tile bits 8..T-1
+                        const int p =
+                            T >= 8 ? (int)((pt.zmask >> (h + 4)) & ((1ull << (T - 8)) - 1)) : 0;
+                        gt.push_back(BTerm{pt.zmask, pt.coefficient * a, pt.coefficient * bb, p, lz});
                     }
+                    if (x == 0)
+                        std::stable_sort(gt.begin(), gt.end(),
+                                         [](const BTerm &u, const BTerm &v) { return u.p < v.p; });
+                    bterms.insert(bterms.end(), gt.begin(), gt.end());
                     groups.push_back(g);
                 }
                 ewins.push_back(ew);

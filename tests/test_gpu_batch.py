@@ -183,3 +183,48 @@ def test_shared_prefixes_with_reused_and_unused_parameters():
             n, r["jx"], r["jy"], r["jz"], r["h"]))
         assert np.abs(gs[i] - g_or).max() < 1e-10
         assert gs[i][-1] == 0.0
+
+
+def _random_observable(n, rng):
+    """Pauli sum with several terms per X mask (odd and even Y counts, Z bits
+    anywhere) and a Z-only group with Z masks over all index bits."""
+    rows = []
+    for _ in range(4):
+        w = int(rng.integers(1, 4))
+        lo = int(rng.integers(0, n - w + 1))
+        x = sum(1 << (lo + k) for k in range(w))
+        for _ in range(int(rng.integers(1, 5))):
+            z = int(rng.integers(0, 1 << n))
+            rows.append((float(rng.normal()), x, z, bin(x & z).count("1")))
+    for _ in range(24):
+        z = int(rng.integers(1, 1 << n))
+        rows.append((float(rng.normal()), 0, z, 0))
+    arr = np.zeros(len(rows), dtype=abi.TERM_DTYPE)
+    for k, (c, x, z, ny) in enumerate(rows):
+        arr[k]["coefficient"] = c
+        arr[k]["xmask"] = np.uint64(x)
+        arr[k]["zmask"] = np.uint64(z)
+        arr[k]["ny"] = ny
+    return arr
+
+
+@pytest.mark.parametrize("tile_bits", [10, 12])
+def test_batch_general_observables_match_plain(tile_bits):
+    """Energy windows with more than two terms per X mask, odd Y counts and a
+    folded Z-only group whose terms spread over every tile bit."""
+    from logosq_b200.batch import BatchedParameterShift
+    rng = np.random.default_rng(17)
+    specs, thetas = [], []
+    for n in (7, 11, 13, 15):
+        gates = workloads.basic_entangling_template(n, 2)
+        terms = _random_observable(n, rng)
+        specs.append((n, gates, 4 * n, terms))
+        thetas.append(rng.uniform(-np.pi, np.pi, 4 * n))
+    b = BatchedParameterShift(specs)
+    call("lq_batch_set_tile_bits", b._h, tile_bits)
+    e, g = b.gradients(np.concatenate(thetas))
+    gs = b.split(g)
+    for i, (n, gates, _, terms) in enumerate(specs):
+        e_plain, g_plain = plain_gradient(n, gates, thetas[i], terms)
+        assert abs(e[i] - e_plain) < 1e-12 * max(1, abs(e_plain)), (n, e[i], e_plain)
+        assert np.abs(gs[i] - g_plain).max() < 1e-10, n
