@@ -269,8 +269,9 @@ def run_vqe_batch(args):
         oracle.set_threads(threads)
         cpu_t, cpu_cost = 0.0, 0.0
         sampled = []
+        small = sorted({r["n"] for r in all_recs})[:2]  # the two smallest qubit counts
         for r in all_recs:
-            if r["n"] in (10, 11) and r["n"] not in sampled:
+            if r["n"] in small and r["n"] not in sampled:
                 sampled.append(r["n"])
                 gates = workloads.basic_entangling_template(r["n"], 4)
                 terms = workloads.heisenberg_terms(r["n"], r["jx"], r["jy"], r["jz"], r["h"])

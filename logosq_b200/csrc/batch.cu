@@ -940,22 +940,42 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
                     return fail(set_error(LQ_ERR_INVALID_ARG, "instance %d term %zu: ny", i, t));
                 byx[pt.xmask].push_back((int)t);
             }
-            // window per group: the first h whose window holds every X bit
-            std::map<int, std::vector<uint64_t>> win;
+            // Windows: every window is one sweep of the state, so take the fewest.
+            // A group's X bits above bit 3 need h in [hi - m + 1, lo] (within
+            // [4, n - m]); points stabbing every such interval, chosen greedily by
+            // right end, are a minimum set.  Groups with no X bit above 3 go to
+            // the first window.
+            struct Need {
+                int a, b;
+                uint64_t x;
+            };
+            std::vector<Need> need;
+            std::vector<uint64_t> free_groups;
             for (auto &kv : byx) {
-                int hsel = -1;
-                for (int h = 4; h + m <= n; ++h)
-                    if ((kv.first & ~window_mask(h, m)) == 0) {
-                        hsel = h;
-                        break;
-                    }
-                if (hsel < 0)
+                const uint64_t up = kv.first & ~0xFull;
+                if (!up) {
+                    free_groups.push_back(kv.first);
+                    continue;
+                }
+                const int lo = __builtin_ctzll(up), hi = 63 - __builtin_clzll(up);
+                const int a = std::max(4, hi - m + 1), bnd = std::min(lo, n - m);
+                if (a > bnd)
                     return fail(set_error(LQ_ERR_UNSUPPORTED,
                                           "instance %d: a Pauli term's X bits span more than "
                                           "one %d-bit window",
                                           i, T));
-                win[hsel].push_back(kv.first);
+                need.push_back(Need{a, bnd, kv.first});
             }
+            std::stable_sort(need.begin(), need.end(),
+                             [](const Need &u, const Need &v) { return u.b < v.b; });
+            std::map<int, std::vector<uint64_t>> win;
+            int cur = -1;
+            for (const Need &q : need) {
+                if (cur < q.a) cur = q.b;
+                win[cur].push_back(q.x);
+            }
+            const int hfree = win.empty() ? 4 : win.begin()->first;
+            for (uint64_t x : free_groups) win[hfree].push_back(x);
             in.ewin_begin = (int)ewins.size();
             for (auto &w : win) {
                 BEWin ew{w.first, (int)groups.size(), (int)w.second.size(), 0};
