@@ -6,7 +6,7 @@
 // Work list: one item per (instance, circuit), circuit 0 unshifted and
 // circuits 2j+1 / 2j+2 with parameter j shifted by +s / -s, ordered by cost
 // (largest qubit count first) and handed out through an atomic counter to
-// persistent CTAs (2 per SM).  Per item a CTA simulates the circuit from
+// persistent CTAs (one per SM).  Per item a CTA simulates the circuit from
 // |0...0> and reduces its FP64 energy:
 //   n <= 12: the whole state lives in the CTA's shared memory (one tile);
 //   n  > 12: the state lives in a per-CTA scratch slot in HBM and is swept in
@@ -18,9 +18,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <map>
 
 #include "fused_plan.h"
+#include "fused_round.cuh"
 
 namespace lq {
 
@@ -70,7 +72,7 @@ struct BItem {
 struct BProgram {  // device program for one fusion width
     int T = 0;
     FusedRound *rounds = nullptr;
-    FusedOp *ops = nullptr;
+    PassOp *ops = nullptr;  // op records (parameter bindings in x0 / x1, see batch_op)
     BPass *passes = nullptr;
     BInst *insts = nullptr;
     std::vector<BInst> h_insts;
@@ -298,10 +300,13 @@ __device__ __forceinline__ void scatter_tile(uint32_t tile_a, double2 *__restric
     }
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 2)
+// One CTA per SM: the ping-pong register rounds hold two 16-amplitude arrays
+// per thread (254 registers without spills); two CTAs per SM at 128 registers
+// spilled and measured slower (2480 vs 2219 ms per 256-instance gradient).
+__global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch(const BItem *__restrict__ items, int nitems, const BInst *__restrict__ insts,
             const BPass *__restrict__ passes, const FusedRound *__restrict__ rounds,
-            const FusedOp *__restrict__ ops, const double *__restrict__ coef,
+            const PassOp *__restrict__ ops, const double *__restrict__ coef,
             const BEWin *__restrict__ ewins, const BGroup *__restrict__ groups,
             const BTerm *__restrict__ terms, double *__restrict__ energy,
             unsigned *__restrict__ counter, double2 *__restrict__ scratch, size_t slot_amps,
@@ -324,11 +329,12 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         const BInst in = insts[item.inst];
         const double *icoef = coef + in.coef_base;
         const int cur_p = item.param, minus = item.sign < 0;
-        auto coef_of = [&](const FusedOp &op) {
-            if (op.param >= 0 && op.param == cur_p)
-                return icoef + op.coef_alt + (minus ? (op.type == F_M2 ? 32 : 8) : 0);
-            if (op.param2 >= 0 && op.param2 == cur_p)
-                return icoef + op.coef_alt2 + (minus ? 8 : 0);
+        // an op bound to the shifted parameter reads its (+s, -s) block
+        auto coef_of = [&](const PassOp &op) {
+            const long long u0 = __double_as_longlong(op.x0), u1 = __double_as_longlong(op.x1);
+            const int p0 = (int)(unsigned)u0, p1 = (int)(unsigned)u1;
+            if (p0 >= 0 && p0 == cur_p) return icoef + (int)(u0 >> 32) + (minus ? 8 : 0);
+            if (p1 >= 0 && p1 == cur_p) return icoef + (int)(u1 >> 32) + (minus ? 8 : 0);
             return icoef + op.coef;
         };
         const int T = in.T;
@@ -372,15 +378,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                     __syncthreads();
                 }
                 for (int r = r0; r < ps.nrounds; ++r) {
-                    // A branch around the round costs the full-width case (all 256
-                    // threads own amplitudes) much of its speed: give it its own
-                    // unconditional copy.
-                    if (nthr == kBatchThreads)
-                        run_round<0>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb,
-                                     ps.h, tid);
-                    else if (tid < nthr)
-                        run_round<0>(tile_a, rounds[ps.round_begin + r], ops, coef_of, tb,
-                                     ps.h, tid);
+                    const FusedRound &rd = rounds[ps.round_begin + r];
+                    // ping-pong register round: every op reads one register array
+                    // and writes the other (no moves at the op dispatch's joins)
+                    if (tid < nthr) {
+                        int tbase = 0;
+                        for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
+                        run_round_pp_sel<0>(tile_a, rd, ops, coef_of, tb, ps.h, tbase);
+                    }
                     __syncthreads();
                     if (base_item) {
                         const int ci = rckpt[ps.round_begin + r];
@@ -578,6 +583,19 @@ static int merge_single_qubit_runs(const std::vector<lq_gate> &gates, int n,
     return LQ_OK;
 }
 
+// The record of a batched op: its 2x2 / X / diagonal / swap code (the ops this
+// engine plans use neither x0 nor x1), and in x0 / x1 the parameters it is bound
+// to with the offsets of their (+s, -s) coefficient blocks, as int32 pairs
+// (parameter, offset); parameter -1: none.
+static PassOp batch_op(const FusedOp &f) {
+    PassOp p = pass_op(f);
+    const int32_t w[4] = {f.param, f.param >= 0 ? f.coef_alt : 0, f.param2,
+                          f.param2 >= 0 ? f.coef_alt2 : 0};
+    std::memcpy(&p.x0, w, 8);
+    std::memcpy(&p.x1, w + 2, 8);
+    return p;
+}
+
 // Build the device program of every instance for fusion width Tw.
 static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     pg.T = Tw;
@@ -620,7 +638,9 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
                 for (int k : rd.ops) {
                     const int gi = st.pass.gates[k];
                     encode_op(gops[gi], st.pass.h, T - 4, rd.rpos, fops, coef_local);
-                    if (fops.back().type == F_M2 || fops.back().type >= F_BLOCK3)
+                    const int ty = fops.back().type;
+                    if (!(ty == F_M1 || ty == F_M1C || ty == F_X || ty == F_XC || ty == F_DIAG ||
+                          ty == F_SWAP))
                         return set_error(LQ_ERR_UNSUPPORTED,
                                          "batched engine: 4x4 gates are not supported");
                     pg.op_members[i].push_back(members[gi]);
@@ -678,12 +698,14 @@ static int build_program(lq_batch *b, int Tw, BProgram &pg) {
     pg.h_rckpt.assign(rounds.size(), -1);
     // energy windows are shared by the programs (set in lq_batch_create)
     LQ_CUDA_TRY(cudaMalloc(&pg.rounds, sizeof(FusedRound) * std::max<size_t>(rounds.size(), 1)));
-    LQ_CUDA_TRY(cudaMalloc(&pg.ops, sizeof(FusedOp) * std::max<size_t>(fops.size(), 1)));
+    std::vector<PassOp> pops;
+    for (const FusedOp &f : fops) pops.push_back(batch_op(f));
+    LQ_CUDA_TRY(cudaMalloc(&pg.ops, sizeof(PassOp) * std::max<size_t>(pops.size(), 1)));
     LQ_CUDA_TRY(cudaMalloc(&pg.passes, sizeof(BPass) * std::max<size_t>(passes.size(), 1)));
     LQ_CUDA_TRY(cudaMalloc(&pg.insts, sizeof(BInst) * pg.h_insts.size()));
     LQ_CUDA_TRY(cudaMemcpy(pg.rounds, rounds.data(), sizeof(FusedRound) * rounds.size(),
                            cudaMemcpyHostToDevice));
-    LQ_CUDA_TRY(cudaMemcpy(pg.ops, fops.data(), sizeof(FusedOp) * fops.size(),
+    LQ_CUDA_TRY(cudaMemcpy(pg.ops, pops.data(), sizeof(PassOp) * pops.size(),
                            cudaMemcpyHostToDevice));
     LQ_CUDA_TRY(cudaMemcpy(pg.passes, passes.data(), sizeof(BPass) * passes.size(),
                            cudaMemcpyHostToDevice));
@@ -910,7 +932,7 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const size_t slots = b->maxn > kSmemStateMax ? (size_t)2 * nsm << b->maxn : 0;
+        const size_t slots = b->maxn > kSmemStateMax ? (size_t)nsm << b->maxn : 0;
         if (b->share_prefix && (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess ||
                                 (need + slots) * sizeof(double2) > freeb / 10 * 8)) {
             b->share_prefix = false;
@@ -1021,7 +1043,7 @@ int lq_batch_create(const lq_vqe_instance *instances, int ninstances, lq_batch *
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    b->grid = 2 * sms;
+    b->grid = sms;  // one resident CTA per SM
     b->slot_amps = b->maxn > kSmemStateMax ? (1ull << b->maxn) : 1;
 #define LQ_B_TRY(x)                                                                 \
     do {                                                                            \

@@ -976,7 +976,7 @@ static int pair_index(int a, int b) {
 }
 
 // The kernel record of one encoded op (flat dispatch code, see PassCode).
-static PassOp pass_op(const FusedOp &f) {
+PassOp pass_op(const FusedOp &f) {
     PassOp p{};
     p.coef = f.coef;
     p.cm = f.cm;

@@ -341,11 +341,12 @@ __device__ __forceinline__ void pp_apply(const double2 (&s)[16], double2 (&d)[16
 // time (a -> b, b -> a), scatter from the array holding the result.
 // tbase is the thread's tile-local base index in this round (its register
 // bits zero), precomputed on the host from the round's lane order.
-template <int MODE>
-__device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &rd,
-                                             const PassOp *__restrict__ ops,
-                                             const double *__restrict__ coef,
-                                             uint64_t tile_base, int h, int tbase) {
+// coef_of(op) gives the op's coefficient pointer (the batched engine swaps in
+// a shifted parameter's coefficients there).
+template <int MODE, class CoefOf>
+__device__ __forceinline__ void run_round_pp_sel(uint32_t tile_a, const FusedRound &rd,
+                                                 const PassOp *__restrict__ ops, CoefOf coef_of,
+                                                 uint64_t tile_base, int h, int tbase) {
     const uint32_t sb = (uint32_t)swz(tbase) << 4;
     const uint64_t gbase = tile_base | (uint64_t)(tbase & 15) | ((uint64_t)(tbase >> 4) << h);
     // The swizzle is linear over XOR, so element e's offset is the XOR of the
@@ -370,19 +371,19 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
         // both records first: the second load is hidden behind the first op
         const PassOp p0 = ops[o];
         const PassOp p1 = ops[o + 1];
-        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
-        pp_apply<MODE>(b, a, p1, coef + p1.coef, gbase, rd.gpos);
+        pp_apply<MODE>(a, b, p0, coef_of(p0), gbase, rd.gpos);
+        pp_apply<MODE>(b, a, p1, coef_of(p1), gbase, rd.gpos);
 #else
         const PassOp p0 = ops[o];
-        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
+        pp_apply<MODE>(a, b, p0, coef_of(p0), gbase, rd.gpos);
         const PassOp p1 = ops[o + 1];
-        pp_apply<MODE>(b, a, p1, coef + p1.coef, gbase, rd.gpos);
+        pp_apply<MODE>(b, a, p1, coef_of(p1), gbase, rd.gpos);
 #endif
     }
     const bool odd = o < o1;
     if (odd) {
         const PassOp p0 = ops[o];
-        pp_apply<MODE>(a, b, p0, coef + p0.coef, gbase, rd.gpos);
+        pp_apply<MODE>(a, b, p0, coef_of(p0), gbase, rd.gpos);
     }
     if (odd) {  // two store paths: no register moves to bring b into a
 #pragma unroll
@@ -398,5 +399,17 @@ __device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &
                          : "memory");
     }
 }
+
+template <int MODE>
+__device__ __forceinline__ void run_round_pp(uint32_t tile_a, const FusedRound &rd,
+                                             const PassOp *__restrict__ ops,
+                                             const double *__restrict__ coef,
+                                             uint64_t tile_base, int h, int tbase) {
+    run_round_pp_sel<MODE>(
+        tile_a, rd, ops, [coef](const PassOp &p) { return coef + p.coef; }, tile_base, h, tbase);
+}
+
+// Host: the record of an encoded op (defined with the fused planner).
+PassOp pass_op(const FusedOp &f);
 
 }  // namespace lq
