@@ -253,9 +253,10 @@ int lq_expectation_pauli(const lq_state *s, const lq_pauli_term *terms, int nter
  * stream (a cudaStream_t, NULL for the default stream) and all scratch lives
  * in one fixed 64 KiB device array inside this library (every GPU that loads
  * the library holds it until the process exits).  At most 1024 terms per call;
- * more returns LQ_ERR_UNSUPPORTED.  The first call on each device looks up the
- * array's device address, so make that first call before any stream capture.
- * Calls share the array: two calls whose work overlaps on the GPU race, so
+ * more returns LQ_ERR_UNSUPPORTED.  The call copies its term table from host
+ * stack memory and waits for its stream, so it cannot be recorded into a CUDA
+ * graph: on a capturing stream it returns LQ_ERR_UNSUPPORTED.  Calls share the
+ * array: two calls whose work overlaps on the GPU race, so
  * serialise them (one stream, or synchronise between them).  The call returns
  * after the result is in *out. */
 int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dtype,

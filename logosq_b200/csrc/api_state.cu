@@ -772,6 +772,14 @@ int lq_expectation_pauli_static(const void *d_amplitudes, int num_qubits, int dt
         if (terms[t].ny != __builtin_popcountll(terms[t].xmask & terms[t].zmask))
             return set_error(LQ_ERR_INVALID_ARG, "Pauli term %d: ny does not match its masks", t);
     }
+    // host-stack copies and a stream wait cannot be captured into a graph
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        LQ_CUDA_TRY(cudaStreamIsCapturing((cudaStream_t)stream, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return set_error(LQ_ERR_UNSUPPORTED,
+                             "lq_expectation_pauli_static cannot run on a capturing stream");
+    }
     // The scratch array is per device: the amplitudes must be on the current one.
     {
         cudaPointerAttributes pa{};

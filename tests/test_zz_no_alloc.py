@@ -113,3 +113,35 @@ def test_static_expectation_rejects_host_pointer():
         call("lq_expectation_pauli_static", buf.ctypes.data_as(C.c_void_p), 4, abi.LQ_C128,
              abi.term_ptr(terms), len(terms), abi.Y_REFERENCE, None, C.byref(out))
     assert e.value.code == abi.LQ_ERR_INVALID_ARG
+
+
+def test_static_refuses_a_capturing_stream():
+    """The call copies its term table from host stack memory and waits for its
+    stream, so it must refuse a stream that is being captured into a graph
+    (and leave the capture intact)."""
+    import torch
+    n = 10
+    st = State.plus_state(n)
+    try:
+        ptr = C.c_void_p()
+        call("lq_state_device_ptr", st.handle, C.byref(ptr))
+        terms = _terms(n, 8, 5)
+        want = _regular(st, terms, abi.Y_REFERENCE)
+        s = torch.cuda.Stream()
+        x = torch.zeros(4, device="cuda")
+        g = torch.cuda.CUDAGraph()
+        out = C.c_double()
+        with torch.cuda.graph(g, stream=s):
+            x.add_(1.0)
+            with pytest.raises(LogosQError) as e:
+                call("lq_expectation_pauli_static", ptr, n, abi.LQ_C128, abi.term_ptr(terms),
+                     len(terms), abi.Y_REFERENCE, C.c_void_p(s.cuda_stream), C.byref(out))
+        assert e.value.code == abi.LQ_ERR_UNSUPPORTED
+        g.replay()
+        torch.cuda.synchronize()
+        assert float(x[0]) == 1.0
+        del g
+        # outside the capture the same call works
+        assert abs(_static(st, terms, abi.Y_REFERENCE) - want) < 1e-12 * max(1, abs(want))
+    finally:
+        st.close()
