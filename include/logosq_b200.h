@@ -348,7 +348,7 @@ int lq_finite_difference(lq_state *work, const lq_gate *ops, int nops, const dou
 
 /* ---------------------------------------------------------------------------
  * Batched parameter-shift engine: all 2P+1 circuits of many VQE instances of
- * uneven qubit counts in one persistent, CUDA-graph-captured launch.
+ * uneven qubit counts in one CUDA-graph-captured call of persistent launches.
  * ------------------------------------------------------------------------- */
 typedef struct lq_vqe_instance {
     int32_t num_qubits;        /* 1..20 */

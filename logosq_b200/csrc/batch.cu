@@ -1,17 +1,19 @@
 // Batched parameter-shift engine: the 2P+1 circuits of many VQE instances
 // (ParameterShift::compute_gradient, src/optimization/gradient.rs:44-78, run
-// for every instance of a batch) in ONE persistent kernel launch, captured in
-// a CUDA graph together with its coefficient upload and result download.
+// for every instance of a batch) in one CUDA graph: coefficient upload, two
+// persistent launches (base circuits, then shifted circuits from the base
+// circuits' checkpoints) and result download.
 //
 // Work list: one item per (instance, circuit), circuit 0 unshifted and
 // circuits 2j+1 / 2j+2 with parameter j shifted by +s / -s, ordered by cost
-// (largest qubit count first) and handed out through an atomic counter to
-// persistent CTAs (one per SM).  Per item a CTA simulates the circuit from
-// |0...0> and reduces its FP64 energy:
+// (largest remaining work first) and handed out through an atomic counter to
+// persistent CTAs (one per SM).  Per item a CTA simulates the circuit (from
+// |0...0>, or from a checkpoint) and reduces its FP64 energy:
 //   n <= 12: the whole state lives in the CTA's shared memory (one tile);
 //   n  > 12: the state lives in a per-CTA scratch slot in HBM and is swept in
 //            2^T-amplitude tiles (T chosen by the autotuner) by the same fused
-//            passes and register rounds as lq_apply_circuit (fused_core.cuh).
+//            passes and ping-pong register rounds as lq_apply_circuit
+//            (fused_round.cuh).
 // Gate coefficients are computed on the host in FP64 with the reference
 // formulas (identical to the plain path); a shifted circuit only swaps in the
 // (+s / -s) coefficients of the ops bound to its parameter.
