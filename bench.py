@@ -554,7 +554,7 @@ def run_qft(args):
                                    f"({len(g)} gates)", "algorithmic_bytes": algo,
                        "l2_policy": "256 MiB written between timed steps (the 16 MiB state "
                                     "starts each step in HBM; later passes find it in L2)"},
-            "roofline": {"kernel": "k_fused_pass", "bound": "hbm",
+            "roofline": {"kernel": "k_fused_pp (fused passes)", "bound": "hbm",
                          "achieved": 2 * S / (launch_ms / 1e3) / 1e9 if f_n else None,
                          "peak": peak, "unit": "GB/s",
                          "frac": 2 * S / (launch_ms / 1e3) / 1e9 / peak if f_n else None,
