@@ -493,6 +493,9 @@ def run_qft(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     res, prof = {}, {}
     sampler = ClockSampler(0)
+    # a 20-qubit step takes well under a millisecond: time enough steps for the
+    # clock sampler (200 ms period) to see the timed region
+    args.steps = max(args.steps, 500)
     for name, mode in (("fused", abi.EXEC_FUSED), ("per_gate", abi.EXEC_PER_GATE)):
         for _ in range(args.warmup):
             st.set_vector(v)
