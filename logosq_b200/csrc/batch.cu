@@ -141,6 +141,7 @@ namespace lq {
 
 constexpr int kBatchThreads = 256;
 constexpr int kSmemStateMax = 12;  // states up to 2^12 amplitudes live in shared memory
+constexpr uint32_t kBatchTileBytes = 16u << kMaxT;  // one tile buffer (two per CTA)
 
 __device__ __forceinline__ uint64_t insert_zero_u(uint64_t x, int pos) {
     const uint64_t lo = x & ((1ull << pos) - 1);
@@ -290,6 +291,25 @@ __device__ __forceinline__ void gather_tile(uint32_t tile_a, const double2 *__re
     }
 }
 
+// The same tile through cp.async (16 bytes per copy, no registers, completes at
+// cp.async.wait_all), so that the next tile streams in while the current one is
+// worked on; src == nullptr writes the state |0...0> directly.
+__device__ __forceinline__ void gather_tile_async(uint32_t tile_a, const double2 *__restrict__ src,
+                                                  int T, int h, uint64_t tile_base, int tid) {
+    if (!src) {
+        gather_tile(tile_a, nullptr, T, h, tile_base, tid);
+        return;
+    }
+    for (int l = tid; l < (1 << T); l += kBatchThreads) {
+        const uint64_t g = tile_base | (uint64_t)(l & 15) | ((uint64_t)(l >> 4) << h);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tile_a +
+                                                                    ((uint32_t)swz(l) << 4)),
+                     "l"(src + g)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 __device__ __forceinline__ void scatter_tile(uint32_t tile_a, double2 *__restrict__ slot, int T,
                                              int h, uint64_t tile_base, int tid) {
     for (int l = tid; l < (1 << T); l += kBatchThreads) {
@@ -373,11 +393,19 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
             // the base circuit's pass-end checkpoint takes the place of the slot
             const int cend = base_item ? rckpt[ps.round_begin + ps.nrounds - 1] : -1;
             double2 *dst = cend >= 0 ? ck + (size_t)cend * N : slot;
+            // two tile buffers: tile t+1 streams in while tile t is worked on (its
+            // amplitudes are disjoint from tile t's, so in-place passes are safe)
+            int buf = 0;
+            if (!in_smem) gather_tile_async(tile_a, src, T, ps.h, tile_base(0, ps.h), tid);
             for (int t = 0; t < ntiles; ++t) {
                 const uint64_t tb = tile_base(t, ps.h);
+                const uint32_t cur = tile_a + (uint32_t)buf * kBatchTileBytes;
                 if (!in_smem) {
-                    gather_tile(tile_a, src, T, ps.h, tb, tid);
+                    asm volatile("cp.async.wait_all;" ::: "memory");
                     __syncthreads();
+                    if (t + 1 < ntiles)
+                        gather_tile_async(tile_a + (uint32_t)(buf ^ 1) * kBatchTileBytes, src, T,
+                                          ps.h, tile_base(t + 1, ps.h), tid);
                 }
                 for (int r = r0; r < ps.nrounds; ++r) {
                     const FusedRound &rd = rounds[ps.round_begin + r];
@@ -386,35 +414,43 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
                     if (tid < nthr) {
                         int tbase = 0;
                         for (int j = 0; j < rd.nlane; ++j) tbase |= ((tid >> j) & 1) << rd.lane[j];
-                        run_round_pp_sel<0>(tile_a, rd, ops, coef_of, tb, ps.h, tbase);
+                        run_round_pp_sel<0>(cur, rd, ops, coef_of, tb, ps.h, tbase);
                     }
                     __syncthreads();
                     if (base_item) {
                         const int ci = rckpt[ps.round_begin + r];
                         if (ci >= 0 && (in_smem || r + 1 < ps.nrounds)) {
-                            scatter_tile(tile_a, ck + (size_t)ci * N, T, ps.h, tb, tid);
+                            scatter_tile(cur, ck + (size_t)ci * N, T, ps.h, tb, tid);
                             __syncthreads();
                         }
                     }
                 }
                 if (!in_smem) {
-                    scatter_tile(tile_a, dst, T, ps.h, tb, tid);
+                    scatter_tile(cur, dst, T, ps.h, tb, tid);
                     __syncthreads();
                 }
+                buf ^= 1;
             }
             if (!in_smem) src = dst;
         }
         for (int w = 0; w < in.newin; ++w) {
             const BEWin ew = ewins[in.ewin_begin + w];
+            int buf = 0;
+            if (!in_smem) gather_tile_async(tile_a, src, T, ew.h, tile_base(0, ew.h), tid);
             for (int t = 0; t < ntiles; ++t) {
                 const uint64_t tb = tile_base(t, ew.h);
+                const uint32_t cur = tile_a + (uint32_t)buf * kBatchTileBytes;
                 if (!in_smem) {
-                    gather_tile(tile_a, src, T, ew.h, tb, tid);
+                    asm volatile("cp.async.wait_all;" ::: "memory");
                     __syncthreads();
+                    if (t + 1 < ntiles)
+                        gather_tile_async(tile_a + (uint32_t)(buf ^ 1) * kBatchTileBytes, src, T,
+                                          ew.h, tile_base(t + 1, ew.h), tid);
                 }
-                acc += tile_energy(tile_a, T, ew.h, tb, groups, ew.group_begin, ew.ngroups, terms,
+                acc += tile_energy(cur, T, ew.h, tb, groups, ew.group_begin, ew.ngroups, terms,
                                    tid);
-                if (!in_smem) __syncthreads();  // before the next gather overwrites the tile
+                if (!in_smem) __syncthreads();  // before a later gather overwrites the tile
+                buf ^= 1;
             }
         }
         // block reduction of the FP64 energy (fixed order)
@@ -431,7 +467,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
     }
 }
 
-static size_t batch_smem() { return (16u << kMaxT) + 2048; }
+static size_t batch_smem() { return 2 * kBatchTileBytes + 2048; }
 
 // 2x2 matrix (m00, m01, m10, m11 as re/im pairs) of an uncontrolled
 // single-qubit op and the index bit it acts on; false for any other op.
