@@ -143,11 +143,6 @@ constexpr int kBatchThreads = 256;
 constexpr int kSmemStateMax = 12;  // states up to 2^12 amplitudes live in shared memory
 constexpr uint32_t kBatchTileBytes = 16u << kMaxT;  // one tile buffer (two per CTA)
 
-__device__ __forceinline__ uint64_t insert_zero_u(uint64_t x, int pos) {
-    const uint64_t lo = x & ((1ull << pos) - 1);
-    return ((x >> pos) << (pos + 1)) | lo;
-}
-
 __device__ __forceinline__ uint32_t insert_zero32(uint32_t x, int pos) {
     return ((x >> pos) << (pos + 1)) | (x & ((1u << pos) - 1));
 }
