@@ -318,7 +318,7 @@ __device__ __forceinline__ void scatter_tile(uint32_t tile_a, double2 *__restric
 }
 
 // One CTA per SM: the ping-pong register rounds hold two 16-amplitude arrays
-// per thread (254 registers without spills); two CTAs per SM at 128 registers
+// per thread (236 registers, no spills); two CTAs per SM at 128 registers
 // spilled and measured slower (2480 vs 2219 ms per 256-instance gradient).
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch(const BItem *__restrict__ items, int nitems, const BInst *__restrict__ insts,
